@@ -1,0 +1,425 @@
+/*
+ * mp_oracle.c -- CPU restatement of the reference's Heisenberg per-gate sweep, used ONLY as test
+ * infrastructure: the parity tests, __graft_entry__.smoke() and bench.py's cpu_baseline leg call it as
+ * the checker. No product code links or calls it.
+ *
+ * Parity is pinned: tests/test_oracle.py checks this restatement bit-for-bit (monomial sets) and to
+ * the last ulp (coefficients) against the unmodified reference engine built by oracle/build_ref.sh, and
+ * against the committed golden fixtures in tests/golden/.
+ *
+ * Semantics restated (reference file:line, paths inside the monoprop project):
+ *   - anticommutation fold: Pauli parity(M & pair_swap(G)) (algebra/PauliAlgebra.h:54-64,80-83);
+ *     Majorana parity(M & G) ^ (|G| odd & |M| odd) (layer_build/Scan.h:221-237, algebra/Algebra.h:70-72).
+ *   - fused cos sweep + emit gate + structural cutoff + upper_atol rescue (layer_build/Scan.h:272-304,
+ *     343-358; CutoffContext.h:20-42; algebra/AlgebraCommon.h:131-176,229-243).
+ *   - rotation phase: Pauli (algebra/PauliAlgebra.h:121-140); Majorana interleave mask times the
+ *     Hermitian phase (algebra/MajoranaAlgebra.h:104-122, algebra/Algebra.h:52-57).
+ *   - leader/follower resolve with the matched set (layer_build/Engine.h:464-513, Common.h:31-48),
+ *     append-only inserts in leader-then-follower order (Engine.h:432-444, MPOperator.h:269-278).
+ *   - rotation apply with the pre-cos partner value recovered as stored*(1/cos)
+ *     (layer_build/FusedApply.h:32-83, Engine.h:209-212,599-614).
+ *   - <0|O|0> = core + sum over fully paired rows of phase*c (MPOperator.h:235-254,
+ *     algebra/PauliAlgebra.h:144-147, algebra/MajoranaAlgebra.h:56-60, MPFunctions.cpp:196-205).
+ *
+ * Bit layout (kept identical to the reference so exported keys compare directly): a monomial over a
+ * storage tier of T modes has 2T bits in W = T/32 little-endian uint64 words; slot s is bit 2T-1-s
+ * (algebra/AlgebraCommon.h:45-52).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MPO_MAXW 8
+#define EVEN_MASK 0x5555555555555555ULL
+#define EMPTY_SLOT 0xFFFFFFFFu
+
+typedef struct {
+    int32_t basis;       /* 0 = majorana, 1 = pauli */
+    int32_t cutoff_type; /* 0 = length, 1 = support */
+    uint32_t cutoff;
+    int32_t has_lower;
+    double lower;
+    int32_t has_upper;
+    double upper;
+    int32_t words; /* W, 1..8 */
+} mpo_config;
+
+typedef struct {
+    mpo_config cfg;
+    size_t n, cap;
+    uint64_t *keys; /* [cap][W] */
+    double *coef;   /* [cap] */
+    uint32_t *table;
+    size_t tcap; /* power of two */
+    uint32_t *mark;
+    uint32_t epoch;
+    double core;
+    uint64_t state_mask[MPO_MAXW];
+} mpo_state;
+
+static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+static uint64_t mix64(uint64_t x) {
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ULL;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebULL;
+    x ^= x >> 31;
+    return x;
+}
+
+static uint64_t key_hash(const uint64_t *k, int W) {
+    uint64_t h = 0;
+    for (int w = 0; w < W; ++w) h ^= mix64(k[w] + (uint64_t)w);
+    return h;
+}
+
+static int key_eq(const uint64_t *a, const uint64_t *b, int W) {
+    for (int w = 0; w < W; ++w)
+        if (a[w] != b[w]) return 0;
+    return 1;
+}
+
+/* Returns the index of key k, or SIZE_MAX. */
+static size_t find(const mpo_state *s, const uint64_t *k) {
+    const int W = s->cfg.words;
+    size_t pos = (size_t)key_hash(k, W) & (s->tcap - 1);
+    for (;;) {
+        uint32_t idx = s->table[pos];
+        if (idx == EMPTY_SLOT) return SIZE_MAX;
+        if (key_eq(s->keys + (size_t)idx * W, k, W)) return idx;
+        pos = (pos + 1) & (s->tcap - 1);
+    }
+}
+
+static void table_put(mpo_state *s, size_t idx) {
+    const int W = s->cfg.words;
+    size_t pos = (size_t)key_hash(s->keys + idx * W, W) & (s->tcap - 1);
+    while (s->table[pos] != EMPTY_SLOT) pos = (pos + 1) & (s->tcap - 1);
+    s->table[pos] = (uint32_t)idx;
+}
+
+static int reserve(mpo_state *s, size_t need) {
+    const int W = s->cfg.words;
+    if (need > s->cap) {
+        size_t nc = s->cap ? s->cap : 1024;
+        while (nc < need) nc *= 2;
+        uint64_t *nk = realloc(s->keys, nc * W * sizeof(uint64_t));
+        if (!nk) return -1;
+        s->keys = nk;
+        double *ncf = realloc(s->coef, nc * sizeof(double));
+        if (!ncf) return -1;
+        s->coef = ncf;
+        uint32_t *nm = realloc(s->mark, nc * sizeof(uint32_t));
+        if (!nm) return -1;
+        memset(nm + s->cap, 0, (nc - s->cap) * sizeof(uint32_t));
+        s->mark = nm;
+        s->cap = nc;
+    }
+    size_t want = 16;
+    while (want < 2 * need) want *= 2;
+    if (want > s->tcap) {
+        free(s->table);
+        s->table = malloc(want * sizeof(uint32_t));
+        if (!s->table) return -1;
+        memset(s->table, 0xFF, want * sizeof(uint32_t));
+        s->tcap = want;
+        for (size_t i = 0; i < s->n; ++i) table_put(s, i);
+    }
+    return 0;
+}
+
+/* --- algebra ------------------------------------------------------------------------------------ */
+
+static void pair_swap(const uint64_t *g, uint64_t *out, int W) {
+    for (int w = 0; w < W; ++w) out[w] = ((g[w] & EVEN_MASK) << 1) | ((g[w] >> 1) & EVEN_MASK);
+}
+
+/* Bit c set iff the number of G bits strictly above c is odd. */
+static void interleave_mask(const uint64_t *g, uint64_t *out, int W) {
+    int above = 0;
+    memset(out, 0, sizeof(uint64_t) * W);
+    for (int c = 64 * W - 1; c >= 0; --c) {
+        if (above & 1) out[c / 64] |= 1ULL << (c % 64);
+        above += (int)((g[c / 64] >> (c % 64)) & 1ULL);
+    }
+}
+
+static int keep_struct(const mpo_state *s, const uint64_t *p, int pop) {
+    const int W = s->cfg.words;
+    /* passes_with_popcount fast path is equivalent: measure <= popcount. */
+    int xs = 0, os = 0;
+    for (int w = 0; w < W; ++w) {
+        uint64_t a = p[w] & EVEN_MASK, b = (p[w] >> 1) & EVEN_MASK;
+        xs += popc(a ^ b);
+        os += popc(a | b);
+    }
+    if (xs == 0) return 1;
+    int measure = s->cfg.cutoff_type == 1 ? os : pop;
+    return measure <= (int)s->cfg.cutoff;
+}
+
+static int is_paired(const uint64_t *p, int W) {
+    for (int w = 0; w < W; ++w)
+        if (((p[w] & EVEN_MASK) ^ ((p[w] >> 1) & EVEN_MASK)) != 0) return 0;
+    return 1;
+}
+
+static int nc2(int n) { return n * (n - 1) / 2; }
+
+typedef struct {
+    uint64_t g[MPO_MAXW], fold[MPO_MAXW], wmask[MPO_MAXW];
+    int gpop, gy, g_odd, pivot_word;
+    uint64_t pivot_bit;
+} gate_ctx;
+
+static void make_ctx(const mpo_state *s, const uint64_t *g, gate_ctx *c) {
+    const int W = s->cfg.words;
+    memcpy(c->g, g, sizeof(uint64_t) * W);
+    c->gpop = 0;
+    c->gy = 0;
+    for (int w = 0; w < W; ++w) {
+        c->gpop += popc(g[w]);
+        uint64_t v = g[w] & EVEN_MASK, u = (g[w] >> 1) & EVEN_MASK;
+        c->gy += popc(v & ~u);
+    }
+    if (s->cfg.basis == 1) {
+        pair_swap(g, c->fold, W);
+        c->g_odd = 0;
+    }
+    else {
+        memcpy(c->fold, g, sizeof(uint64_t) * W);
+        c->g_odd = c->gpop & 1;
+        interleave_mask(g, c->wmask, W);
+    }
+    c->pivot_word = -1;
+    c->pivot_bit = 0;
+    for (int w = 0; w < W; ++w) {
+        if (g[w]) {
+            c->pivot_word = w;
+            c->pivot_bit = g[w] & (~g[w] + 1);
+            break;
+        }
+    }
+}
+
+static int phase_of(const mpo_state *s, const gate_ctx *c, const uint64_t *m, const uint64_t *p, int mpop, int ov) {
+    const int W = s->cfg.words;
+    if (s->cfg.basis == 1) {
+        long e = c->gy, cross = 0;
+        for (int w = 0; w < W; ++w) {
+            uint64_t vm = m[w] & EVEN_MASK, um = (m[w] >> 1) & EVEN_MASK;
+            uint64_t vn = p[w] & EVEN_MASK, un = (p[w] >> 1) & EVEN_MASK;
+            uint64_t vg = c->g[w] & EVEN_MASK, ug = (c->g[w] >> 1) & EVEN_MASK;
+            e += popc(vm & ~um);
+            e -= popc(vn & ~un);
+            cross += popc(vm & (ug ^ vg));
+        }
+        long t = e + 2 * cross;
+        return (((t % 4) + 4) % 4) == 1 ? -1 : 1;
+    }
+    int par = 0;
+    for (int w = 0; w < W; ++w) par ^= popc(m[w] & c->wmask[w]) & 1;
+    static const int REAL[4] = {1, 0, -1, 0};
+    int ppop = mpop + c->gpop - 2 * ov;
+    int power = (nc2(mpop) + nc2(c->gpop) - nc2(ppop) + 3) % 4;
+    return (par ? -1 : 1) * REAL[power];
+}
+
+/* --- public ABI ----------------------------------------------------------------------------------- */
+
+typedef struct {
+    size_t src;
+    uint64_t p[MPO_MAXW];
+    int phase;
+    double v;
+} query;
+
+void *mpo_create(const mpo_config *cfg,
+                 size_t n_terms,
+                 const uint64_t *words,
+                 const double *coefs,
+                 double core,
+                 const uint64_t *state_mask) {
+    if (cfg->words < 1 || cfg->words > MPO_MAXW) return NULL;
+    mpo_state *s = calloc(1, sizeof(mpo_state));
+    if (!s) return NULL;
+    s->cfg = *cfg;
+    s->core = core;
+    memcpy(s->state_mask, state_mask, sizeof(uint64_t) * cfg->words);
+    if (reserve(s, n_terms ? n_terms : 1) != 0) return NULL;
+    const int W = cfg->words;
+    for (size_t i = 0; i < n_terms; ++i) {
+        memcpy(s->keys + s->n * W, words + i * W, sizeof(uint64_t) * W);
+        s->coef[s->n] = coefs[i];
+        table_put(s, s->n);
+        s->n++;
+    }
+    return s;
+}
+
+/* Applies gates[n_gates-1] .. gates[0] (Heisenberg order, MonomialPropagator.inl:720-733).
+ * gen_words: [n_gates][W]; angles: theta[map]*g per gate, in circuit order.
+ * counts (optional): per APPLIED gate (application order) {n_g, a_g, e_g, m_g}. */
+int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const double *angles, uint64_t *counts) {
+    mpo_state *s = hs;
+    const int W = s->cfg.words;
+    query *qs = NULL;
+    size_t qcap = 0;
+    size_t *miss = NULL;
+    for (size_t step = 0; step < n_gates; ++step) {
+        const size_t gi = n_gates - 1 - step;
+        const uint64_t *g = gen_words + gi * W;
+        const double ang = angles[gi];
+        const double cosv = cos(2.0 * ang);
+        const double sinv = sin(2.0 * ang);
+        const double abs_sin = fabs(sinv);
+        const int fused = cosv != 0.0;
+        const double inv_cos = fused ? 1.0 / cosv : 1.0;
+        gate_ctx c;
+        make_ctx(s, g, &c);
+        const size_t n0 = s->n;
+        if (qcap < n0 + 1) {
+            qcap = 2 * (n0 + 1);
+            qs = realloc(qs, qcap * sizeof(query));
+            miss = realloc(miss, qcap * sizeof(size_t));
+            if (!qs || !miss) return -1;
+        }
+        size_t n_anti = 0, nl = 0, nf = 0;
+        /* queries: leaders in [0, nl), followers stored from the top down: [qcap-nf, qcap) */
+        if (c.pivot_word >= 0) {
+            for (size_t i = 0; i < n0; ++i) {
+                const uint64_t *m = s->keys + i * W;
+                int par = 0, mpop = 0;
+                for (int w = 0; w < W; ++w) {
+                    par ^= popc(m[w] & c.fold[w]) & 1;
+                    mpop += popc(m[w]);
+                }
+                if (c.g_odd) par ^= mpop & 1;
+                if (!par) continue;
+                ++n_anti;
+                const double v = s->coef[i];
+                if (fused) s->coef[i] = v * cosv;
+                const double av = fabs(v);
+                if (s->cfg.has_lower && abs_sin * av <= s->cfg.lower) continue;
+                uint64_t p[MPO_MAXW];
+                int ov = 0;
+                for (int w = 0; w < W; ++w) {
+                    p[w] = m[w] ^ g[w];
+                    ov += popc(m[w] & g[w]);
+                }
+                const int ppop = mpop + c.gpop - 2 * ov;
+                const int keep = keep_struct(s, p, ppop);
+                if (!keep && !(s->cfg.has_upper && abs_sin * av >= s->cfg.upper)) continue;
+                const int ph = phase_of(s, &c, m, p, mpop, ov);
+                const int follower = (m[c.pivot_word] & c.pivot_bit) != 0;
+                query *q = follower ? &qs[qcap - 1 - nf++] : &qs[nl++];
+                q->src = i;
+                memcpy(q->p, p, sizeof(uint64_t) * W);
+                q->phase = ph;
+                q->v = v;
+            }
+        }
+        /* resolve: leaders then followers (followers in ascending source order) */
+        s->epoch++;
+        size_t n_miss = 0;
+        double *c_arr = s->coef;
+        /* Hits are applied after both passes; record them in place of the query (reuse fields). */
+        typedef struct {
+            size_t src, tgt;
+            int phase;
+            double vs, vt;
+        } hit;
+        hit *hits = malloc((nl + nf + 1) * sizeof(hit));
+        size_t nh = 0;
+        for (size_t k = 0; k < nl + nf; ++k) {
+            const int is_leader = k < nl;
+            /* followers were pushed top-down; read them back in ascending source order */
+            query *q = is_leader ? &qs[k] : &qs[qcap - 1 - (k - nl)];
+            if (!is_leader && s->mark[q->src] == s->epoch) continue;
+            size_t j = find(s, q->p);
+            if (j != SIZE_MAX && j < n0) {
+                if (is_leader) s->mark[j] = s->epoch;
+                hit h = {q->src, j, q->phase, q->v, fused ? c_arr[j] * inv_cos : c_arr[j]};
+                hits[nh++] = h;
+            }
+            else {
+                miss[n_miss++] = (size_t)(q - qs);
+            }
+        }
+        if (reserve(s, n0 + n_miss) != 0) return -1;
+        c_arr = s->coef;
+        if (!fused) {
+            /* two-pass form (cos == 0): every anticommuting term is scaled before the adds */
+            for (size_t i = 0; i < n0; ++i) {
+                const uint64_t *m = s->keys + i * W;
+                int par = 0, mpop = 0;
+                for (int w = 0; w < W; ++w) {
+                    par ^= popc(m[w] & c.fold[w]) & 1;
+                    mpop += popc(m[w]);
+                }
+                if (c.g_odd) par ^= mpop & 1;
+                if (par) c_arr[i] = cosv * c_arr[i];
+            }
+        }
+        for (size_t k = 0; k < nh; ++k) {
+            const hit *h = &hits[k];
+            c_arr[h->src] += sinv * (double)(-h->phase) * h->vt;
+            c_arr[h->tgt] += sinv * (double)(h->phase) * h->vs;
+        }
+        for (size_t k = 0; k < n_miss; ++k) {
+            const query *q = &qs[miss[k]];
+            const size_t idx = s->n++;
+            memcpy(s->keys + idx * W, q->p, sizeof(uint64_t) * W);
+            c_arr[idx] = sinv * (double)q->phase * q->v;
+            table_put(s, idx);
+        }
+        free(hits);
+        if (counts) {
+            counts[4 * step + 0] = n0;
+            counts[4 * step + 1] = n_anti;
+            counts[4 * step + 2] = nl + nf;
+            counts[4 * step + 3] = n_miss;
+        }
+    }
+    free(qs);
+    free(miss);
+    return 0;
+}
+
+size_t mpo_size(void *hs) { return ((mpo_state *)hs)->n; }
+
+void mpo_export(void *hs, uint64_t *words, double *coefs) {
+    mpo_state *s = hs;
+    memcpy(words, s->keys, s->n * s->cfg.words * sizeof(uint64_t));
+    memcpy(coefs, s->coef, s->n * sizeof(double));
+}
+
+double mpo_expectation(void *hs) {
+    mpo_state *s = hs;
+    const int W = s->cfg.words;
+    double acc = 0.0;
+    for (size_t i = 0; i < s->n; ++i) {
+        const uint64_t *m = s->keys + i * W;
+        if (!is_paired(m, W)) continue;
+        int na = 0, pop = 0;
+        for (int w = 0; w < W; ++w) {
+            na += popc(m[w] & s->state_mask[w]);
+            pop += popc(m[w]);
+        }
+        int odd = s->cfg.basis == 1 ? (na & 1) : ((na + pop / 2) & 1);
+        acc += (odd ? -1.0 : 1.0) * s->coef[i];
+    }
+    return s->core + acc;
+}
+
+void mpo_destroy(void *hs) {
+    mpo_state *s = hs;
+    if (!s) return;
+    free(s->keys);
+    free(s->coef);
+    free(s->table);
+    free(s->mark);
+    free(s);
+}
