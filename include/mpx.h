@@ -1,0 +1,135 @@
+/*
+ * mpx.h -- C ABI of the B200 propagation engine (libmpx.so).
+ *
+ * Plain C types only. Caller-owned host buffers are borrowed for the duration of a call; the device
+ * term store is owned by the handle. One CUDA stream per handle; a handle is not thread-safe. Every
+ * entry point returns an mpx_status; mpx_last_error() gives the message of the handle's last failure
+ * (or of the last failed mpx_create on this thread when the handle is NULL).
+ *
+ * Each entry point replaces one method of the reference's per-tier engine class, reached from Python
+ * through its nanobind module (src/monoprop/bindings/binder.h) and implemented in C++ by
+ * MonomialPropagator<NumModes> (cpp/include/monoprop/MonomialPropagator.h); citations are to those files.
+ *
+ * Key layout (identical to the reference's, so keys compare word for word): a monomial over a storage
+ * tier of T = ceil(num_modes/32)*32 modes is 2T bits in W = T/32 little-endian uint64 words, slot s at
+ * bit 2T-1-s (cpp/monoprop/algebra/AlgebraCommon.h:45-52).
+ */
+#ifndef MPX_H
+#define MPX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPX_API __attribute__((visibility("default")))
+#else
+#define MPX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MPX_OK = 0,
+    MPX_ERR_INVALID = 1,  /* bad argument: reference raises ValueError / std::invalid_argument */
+    MPX_ERR_CUDA = 2,     /* CUDA runtime error (message carries cudaGetErrorString) */
+    MPX_ERR_NOMEM = 3,    /* device allocation failed */
+    MPX_ERR_CAPACITY = 4, /* a bounded resource (fixed arena) is too small for the request */
+    MPX_ERR_STATE = 5,    /* call not valid in the engine's current state: RuntimeError */
+    MPX_ERR_NO_DEVICE = 6 /* no CUDA device / the sm_100a kernels cannot run here */
+} mpx_status;
+
+typedef enum { MPX_BASIS_MAJORANA = 0, MPX_BASIS_PAULI = 1 } mpx_basis;
+typedef enum { MPX_CUTOFF_LENGTH = 0, MPX_CUTOFF_SUPPORT = 1 } mpx_cutoff_type;
+
+typedef struct {
+    int32_t basis;       /* mpx_basis; reference ctor kwarg basis= (binder.h:61-101) */
+    int32_t cutoff_type; /* mpx_cutoff_type; kwarg cutoff_type= */
+    uint32_t cutoff;     /* kwarg cutoff= */
+    int32_t has_lower_atol;
+    double lower_atol; /* kwarg lower_atol= (valid iff has_lower_atol) */
+    int32_t has_upper_atol;
+    double upper_atol;     /* kwarg upper_atol= (valid iff has_upper_atol) */
+    int32_t num_modes;     /* logical modes (qubits in the Pauli basis); kwarg logical_num_modes= */
+    int32_t device;        /* CUDA device ordinal */
+    uint64_t capacity_hint; /* initial term capacity; 0 = automatic. The store grows on demand. */
+} mpx_config;
+
+typedef struct mpx_engine mpx_engine;
+
+/* Construct the Heisenberg term store from an encoded observable.
+ * Replaces MonomialPropagator<N>::MonomialPropagator (MonomialPropagator.h:73-84; body
+ * MonomialPropagator.inl:73-188). obs_words: [n_obs][W] distinct non-empty keys; obs_coef: encoded real
+ * coefficients (Pauli: real part; Majorana: coeff / i^C(|M|,2)); core: the encoded empty-monomial
+ * coefficient; state_mask: [W] key with slot 2m set for every occupied mode m of the reference state. */
+MPX_API mpx_status mpx_create(const mpx_config *cfg,
+                      const uint64_t *obs_words,
+                      const double *obs_coef,
+                      uint64_t n_obs,
+                      double core,
+                      const uint64_t *state_mask,
+                      mpx_engine **out);
+
+/* Heisenberg propagation: applies gen_words[n_layers-1] first down to gen_words[0], each rotation
+ * exp(+i angle G) with angle = theta[mapping]*gen_coeff already mapped (MPFunctions.cpp:57-69).
+ * Replaces MonomialPropagator<N>::propagate (MonomialPropagator.h:121-125, .inl:692-718).
+ * gen_words: [n_layers][W]. Host buffers. */
+MPX_API mpx_status mpx_propagate(mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n_layers);
+
+/* A circuit uploaded once to device memory as per-gate descriptors, for repeated propagation (the
+ * reference re-expands the circuit on every call: monomial_propagator.py:257-283). Angles can be
+ * replaced without re-uploading the generators. */
+typedef struct mpx_circuit mpx_circuit;
+MPX_API mpx_status mpx_circuit_upload(mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n_layers,
+                              mpx_circuit **out);
+MPX_API mpx_status mpx_circuit_set_angles(mpx_engine *e, mpx_circuit *c, const double *angles);
+MPX_API mpx_status mpx_propagate_circuit(mpx_engine *e, const mpx_circuit *c);
+MPX_API void mpx_circuit_destroy(mpx_circuit *c);
+
+/* <0|O|0> of the current operator: core + sum of phase*c over fully paired terms.
+ * Replaces MonomialPropagator<N>::expectation_value with empty parameters (.inl:1034-1041,
+ * MPFunctions.cpp:196-205). */
+MPX_API mpx_status mpx_expectation(mpx_engine *e, double *out);
+
+/* Number of terms in the store. Replaces MonomialPropagator<N>::size (MonomialPropagator.h:100). */
+MPX_API mpx_status mpx_size(mpx_engine *e, uint64_t *out);
+
+/* Words per key (W). */
+MPX_API mpx_status mpx_words(mpx_engine *e, uint32_t *out);
+
+/* Raw export of every stored key and its FP64 coefficient, in storage order, up to cap terms.
+ * Replaces the raw read behind MonomialPropagator<N>::evolved_operator_terms (.inl:1099-1127) before its
+ * atol filter, decoding and 1e-12 rounding (those stay on the host side). */
+MPX_API mpx_status mpx_export(mpx_engine *e, uint64_t *words, double *coefs, uint64_t cap, uint64_t *n_out);
+
+/* Per applied gate of the last propagate call, in application order: {n_g, a_g, e_g, m_g} =
+ * terms before the gate, anticommuting terms, emitted sine branches, appended terms. */
+MPX_API mpx_status mpx_gate_stats(mpx_engine *e, uint64_t *out4, uint64_t max_gates, uint64_t *n_out);
+
+/* Restore the operator the engine was created with (keeps allocations). */
+MPX_API mpx_status mpx_reset(mpx_engine *e);
+
+/* Setters mirroring the reference properties (binder.h:154-185; MonomialPropagator.h:168-211). */
+MPX_API mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff);
+MPX_API mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value);
+MPX_API mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value);
+
+/* Device pointers of the live store (keys [n][W], coefficients [n]) for in-process consumers such as
+ * the torch wrapper; valid until the next mutating call. */
+MPX_API mpx_status mpx_device_view(mpx_engine *e, const uint64_t **keys, double **coefs, uint64_t *n);
+
+/* CUDA stream (cudaStream_t, as void*) the engine launches on. */
+MPX_API mpx_status mpx_stream(mpx_engine *e, void **stream);
+
+/* Number of engine kernel launches issued since the engine was created. */
+MPX_API mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out);
+
+MPX_API const char *mpx_last_error(const mpx_engine *e);
+MPX_API void mpx_destroy(mpx_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPX_H */

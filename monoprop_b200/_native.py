@@ -1,0 +1,249 @@
+"""ctypes binding of the engine's C ABI (``include/mpx.h``, ``monoprop_b200/libmpx.so``).
+
+This is the thin host layer every Python caller goes through. There is no CPU fallback: if the library
+is missing or no sm_100a device is visible, constructing an :class:`Engine` raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmpx.so")
+
+MPX_OK = 0
+_STATUS = {1: "MPX_ERR_INVALID", 2: "MPX_ERR_CUDA", 3: "MPX_ERR_NOMEM", 4: "MPX_ERR_CAPACITY", 5: "MPX_ERR_STATE",
+           6: "MPX_ERR_NO_DEVICE"}
+
+#: Every entry point declared in include/mpx.h.
+EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_set_angles", "mpx_propagate_circuit",
+            "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
+            "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
+            "mpx_stream", "mpx_launch_count", "mpx_last_error", "mpx_destroy")
+
+
+class MpxError(RuntimeError):
+    """An engine call failed; ``status`` is the mpx_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class MpxInvalid(MpxError, ValueError):
+    """MPX_ERR_INVALID: the reference raises ValueError for these."""
+
+
+class Config(C.Structure):
+    _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
+                ("has_lower_atol", C.c_int32), ("lower_atol", C.c_double), ("has_upper_atol", C.c_int32),
+                ("upper_atol", C.c_double), ("num_modes", C.c_int32), ("device", C.c_int32),
+                ("capacity_hint", C.c_uint64)]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libmpx.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m monoprop_b200.build` "
+                              "(the engine has no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        vp, u64, st = C.c_void_p, C.c_uint64, C.c_int
+        sig = {
+            "mpx_create": (st, [C.POINTER(Config), vp, vp, u64, C.c_double, vp, C.POINTER(vp)]),
+            "mpx_propagate": (st, [vp, vp, vp, u64]),
+            "mpx_circuit_upload": (st, [vp, vp, vp, u64, C.POINTER(vp)]),
+            "mpx_circuit_set_angles": (st, [vp, vp, vp]),
+            "mpx_propagate_circuit": (st, [vp, vp]),
+            "mpx_circuit_destroy": (None, [vp]),
+            "mpx_expectation": (st, [vp, C.POINTER(C.c_double)]),
+            "mpx_size": (st, [vp, C.POINTER(u64)]),
+            "mpx_words": (st, [vp, C.POINTER(C.c_uint32)]),
+            "mpx_export": (st, [vp, vp, vp, u64, C.POINTER(u64)]),
+            "mpx_gate_stats": (st, [vp, vp, u64, C.POINTER(u64)]),
+            "mpx_reset": (st, [vp]),
+            "mpx_set_cutoff": (st, [vp, C.c_uint32]),
+            "mpx_set_lower_atol": (st, [vp, C.c_int32, C.c_double]),
+            "mpx_set_upper_atol": (st, [vp, C.c_int32, C.c_double]),
+            "mpx_device_view": (st, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]),
+            "mpx_stream": (st, [vp, C.POINTER(vp)]),
+            "mpx_launch_count": (st, [vp, C.POINTER(u64)]),
+            "mpx_last_error": (C.c_char_p, [vp]),
+            "mpx_destroy": (None, [vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray) -> C.c_void_p:
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class GateStats:
+    """Per applied gate (application order): terms before, anticommuting, emitted, appended."""
+
+    n: np.ndarray
+    anti: np.ndarray
+    emitted: np.ndarray
+    appended: np.ndarray
+
+    @property
+    def term_gate_updates(self) -> int:
+        return int(self.n.sum())
+
+
+class Circuit:
+    """A circuit resident in device memory (``mpx_circuit``)."""
+
+    def __init__(self, engine: Engine, gen_words: np.ndarray, angles: np.ndarray):
+        self.engine = engine
+        gw = np.ascontiguousarray(gen_words, dtype=np.uint64)
+        an = np.ascontiguousarray(angles, dtype=np.float64)
+        if gw.ndim != 2 or gw.shape[0] != an.shape[0] or gw.shape[1] != engine.words:
+            raise ValueError("gen_words must be [n_layers, W] and angles [n_layers]")
+        self.n_layers = gw.shape[0]
+        h = C.c_void_p()
+        engine._check(engine.lib.mpx_circuit_upload(engine.h, _p(gw), _p(an), self.n_layers, C.byref(h)))
+        self.h = h
+
+    def set_angles(self, angles: np.ndarray) -> None:
+        an = np.ascontiguousarray(angles, dtype=np.float64)
+        if an.shape != (self.n_layers,):
+            raise ValueError("angles must have one entry per layer")
+        self.engine._check(self.engine.lib.mpx_circuit_set_angles(self.engine.h, self.h, _p(an)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.engine.lib.mpx_circuit_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """One device-resident Heisenberg term store (``mpx_engine``)."""
+
+    def __init__(self, *, basis: str, cutoff_type: str, cutoff: int, num_modes: int,
+                 keys: np.ndarray, coefs: np.ndarray, core: float, state_mask: np.ndarray,
+                 lower_atol: float | None = None, upper_atol: float | None = None, device: int = 0,
+                 capacity_hint: int = 0):
+        self.lib = load()
+        cfg = Config(1 if basis == "pauli" else 0, 1 if cutoff_type == "support" else 0, int(cutoff),
+                     int(lower_atol is not None), float(lower_atol or 0.0), int(upper_atol is not None),
+                     float(upper_atol or 0.0), int(num_modes), int(device), int(capacity_hint))
+        self.words = (int(num_modes) + 31) // 32
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, self.words)
+        c = np.ascontiguousarray(coefs, dtype=np.float64).reshape(-1)
+        m = np.ascontiguousarray(state_mask, dtype=np.uint64).reshape(-1)
+        if k.shape[0] != c.shape[0]:
+            raise ValueError("keys and coefs disagree in length")
+        if m.shape[0] < self.words:
+            m = np.concatenate([m, np.zeros(self.words - m.shape[0], np.uint64)])
+        h = C.c_void_p()
+        rc = self.lib.mpx_create(C.byref(cfg), _p(k) if k.size else None, _p(c) if c.size else None, k.shape[0],
+                                 float(core), _p(m), C.byref(h))
+        if rc != MPX_OK:
+            msg = self.lib.mpx_last_error(None).decode()
+            raise (MpxInvalid if rc == 1 else MpxError)(rc, msg)
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != MPX_OK:
+            msg = self.lib.mpx_last_error(self.h).decode()
+            raise (MpxInvalid if rc == 1 else MpxError)(rc, msg)
+
+    def propagate(self, gen_words: np.ndarray, angles: np.ndarray) -> None:
+        gw = np.ascontiguousarray(gen_words, dtype=np.uint64).reshape(-1, self.words)
+        an = np.ascontiguousarray(angles, dtype=np.float64).reshape(-1)
+        if gw.shape[0] != an.shape[0]:
+            raise ValueError("one angle per generator is required")
+        self._check(self.lib.mpx_propagate(self.h, _p(gw), _p(an), gw.shape[0]))
+
+    def upload(self, gen_words: np.ndarray, angles: np.ndarray) -> Circuit:
+        return Circuit(self, gen_words, angles)
+
+    def propagate_circuit(self, circuit: Circuit) -> None:
+        self._check(self.lib.mpx_propagate_circuit(self.h, circuit.h))
+
+    def expectation(self) -> float:
+        out = C.c_double(0.0)
+        self._check(self.lib.mpx_expectation(self.h, C.byref(out)))
+        return out.value
+
+    def size(self) -> int:
+        out = C.c_uint64(0)
+        self._check(self.lib.mpx_size(self.h, C.byref(out)))
+        return int(out.value)
+
+    def export(self) -> tuple[np.ndarray, np.ndarray]:
+        n = self.size()
+        keys = np.zeros((max(n, 1), self.words), dtype=np.uint64)
+        coefs = np.zeros(max(n, 1), dtype=np.float64)
+        got = C.c_uint64(0)
+        self._check(self.lib.mpx_export(self.h, _p(keys), _p(coefs), n, C.byref(got)))
+        return keys[:n], coefs[:n]
+
+    def gate_stats(self) -> GateStats:
+        n = C.c_uint64(0)
+        self._check(self.lib.mpx_gate_stats(self.h, None, 0, C.byref(n)))
+        out = np.zeros((max(int(n.value), 1), 4), dtype=np.uint64)
+        self._check(self.lib.mpx_gate_stats(self.h, _p(out), int(n.value), C.byref(n)))
+        out = out[: int(n.value)]
+        return GateStats(out[:, 0].copy(), out[:, 1].copy(), out[:, 2].copy(), out[:, 3].copy())
+
+    def reset(self) -> None:
+        self._check(self.lib.mpx_reset(self.h))
+
+    def set_cutoff(self, cutoff: int) -> None:
+        self._check(self.lib.mpx_set_cutoff(self.h, int(cutoff)))
+
+    def set_lower_atol(self, value: float | None) -> None:
+        self._check(self.lib.mpx_set_lower_atol(self.h, int(value is not None), float(value or 0.0)))
+
+    def set_upper_atol(self, value: float | None) -> None:
+        self._check(self.lib.mpx_set_upper_atol(self.h, int(value is not None), float(value or 0.0)))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self.lib.mpx_stream(self.h, C.byref(s)))
+        return int(s.value or 0)
+
+    def launch_count(self) -> int:
+        out = C.c_uint64(0)
+        self._check(self.lib.mpx_launch_count(self.h, C.byref(out)))
+        return int(out.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mpx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def engine_for(wl, **kw) -> Engine:
+    """Engine holding workload ``wl``'s observable (see :mod:`monoprop_b200.workloads`)."""
+    keys, coefs, core = wl.encoded_observable()
+    return Engine(basis=wl.basis, cutoff_type=wl.cutoff_type, cutoff=wl.cutoff, num_modes=wl.num_modes,
+                  keys=keys, coefs=coefs, core=core, state_mask=wl.state_mask(), lower_atol=wl.lower_atol,
+                  upper_atol=wl.upper_atol, **kw)

@@ -1,0 +1,719 @@
+// mpx_engine.cu -- host engine and C ABI (include/mpx.h) of the B200 propagation engine.
+//
+// The engine owns one CUDA stream and a device-resident term store. A propagate call uploads the
+// circuit once as per-gate descriptors, then issues two kernels per gate with no host round trip per
+// gate: the sweep kernel refuses to start a gate that could overflow the store (it records the step and
+// every later launch becomes a no-op), and the host, which checks the counters once per chunk of gates,
+// grows the store and re-issues from that step. Truncation semantics follow the reference's fused
+// ContractImmediately path (MonomialPropagator.inl:594-618).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mpx.h"
+#include "mpx_kernels.cuh"
+
+using namespace mpx;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct mpx_circuit {
+    mpx::GateDesc *d_desc = nullptr;
+    uint64_t n = 0;
+    std::vector<uint64_t> words; // host copy of the generators, for mpx_circuit_set_angles
+    int W = 1;
+    int device = 0;
+};
+using CircuitDev = mpx_circuit;
+
+struct mpx_engine {
+    mpx_config cfg{};
+    int W = 1;
+    Trunc tr{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int grid = 0;
+    Store st{};
+    Scratch sc{};
+    Counters *d_cnt = nullptr;
+    Counters *h_cnt = nullptr; // pinned
+    Counters *h_snap = nullptr; // pinned, two per-chunk snapshots
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    StateMask mask{};
+    double core = 0.0;
+    uint64_t *d_init_keys = nullptr;
+    double *d_init_coef = nullptr;
+    uint64_t n_init = 0;
+    uint64_t *d_stats = nullptr;
+    uint64_t stats_cap = 0;
+    uint64_t last_gates = 0;
+    std::vector<uint64_t> h_stats;
+    double *d_partial = nullptr;
+    double *d_out = nullptr;
+    double *h_out = nullptr; // pinned
+    uint64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+#define MPX_CUDA(call)                                                                                              \
+    do {                                                                                                            \
+        cudaError_t e_ = (call);                                                                                    \
+        if (e_ != cudaSuccess) {                                                                                    \
+            return fail(eng, MPX_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));                      \
+        }                                                                                                           \
+    } while (0)
+
+mpx_status fail(mpx_engine *eng, mpx_status st, const std::string &msg) {
+    if (eng != nullptr) eng->err = msg;
+    else g_create_error = msg;
+    return st;
+}
+
+uint64_t next_pow2(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// ----- kernel dispatch over (W, basis) ------------------------------------------------------------------
+
+template <int W, int B>
+void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
+    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr);
+    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats);
+}
+
+template <int W, int B>
+void launch_expect(mpx_engine *e) {
+    k_expect<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, e->mask, e->d_partial);
+}
+
+template <int W>
+void launch_build(mpx_engine *e, uint64_t lo, uint64_t hi) {
+    if (hi <= lo) return;
+    const uint64_t blocks = std::min<uint64_t>((hi - lo + 255) / 256, static_cast<uint64_t>(e->grid) * 4);
+    k_build_table<W><<<static_cast<unsigned>(blocks), 256, 0, e->stream>>>(e->st, e->d_cnt, lo, hi);
+}
+
+using GateFn = void (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t);
+using ExpFn = void (*)(mpx_engine *);
+using BuildFn = void (*)(mpx_engine *, uint64_t, uint64_t);
+
+template <int W>
+GateFn gate_fn(int basis) {
+    return basis == 1 ? &launch_gate<W, 1> : &launch_gate<W, 0>;
+}
+template <int W>
+ExpFn exp_fn(int basis) {
+    return basis == 1 ? &launch_expect<W, 1> : &launch_expect<W, 0>;
+}
+
+GateFn pick_gate(int W, int basis) {
+    switch (W) {
+    case 1: return gate_fn<1>(basis);
+    case 2: return gate_fn<2>(basis);
+    case 3: return gate_fn<3>(basis);
+    case 4: return gate_fn<4>(basis);
+    case 5: return gate_fn<5>(basis);
+    case 6: return gate_fn<6>(basis);
+    case 7: return gate_fn<7>(basis);
+    default: return gate_fn<8>(basis);
+    }
+}
+ExpFn pick_exp(int W, int basis) {
+    switch (W) {
+    case 1: return exp_fn<1>(basis);
+    case 2: return exp_fn<2>(basis);
+    case 3: return exp_fn<3>(basis);
+    case 4: return exp_fn<4>(basis);
+    case 5: return exp_fn<5>(basis);
+    case 6: return exp_fn<6>(basis);
+    case 7: return exp_fn<7>(basis);
+    default: return exp_fn<8>(basis);
+    }
+}
+BuildFn pick_build(int W) {
+    switch (W) {
+    case 1: return &launch_build<1>;
+    case 2: return &launch_build<2>;
+    case 3: return &launch_build<3>;
+    case 4: return &launch_build<4>;
+    case 5: return &launch_build<5>;
+    case 6: return &launch_build<6>;
+    case 7: return &launch_build<7>;
+    default: return &launch_build<8>;
+    }
+}
+
+// ----- store management ---------------------------------------------------------------------------------
+
+void free_store(mpx_engine *e) {
+    cudaFree(e->st.keys);
+    cudaFree(e->st.coef);
+    cudaFree(e->st.table);
+    cudaFree(e->sc.q_src);
+    cudaFree(e->sc.q_flag);
+    cudaFree(e->sc.q_val);
+    cudaFree(e->sc.emit_bits);
+    cudaFree(e->sc.aux);
+    e->st = Store{};
+    e->sc.q_src = nullptr;
+    e->sc.q_flag = nullptr;
+    e->sc.q_val = nullptr;
+    e->sc.emit_bits = nullptr;
+    e->sc.aux = nullptr;
+}
+
+// (Re)allocates the store for capacity `cap`, keeping the first n terms, and rebuilds the hash table.
+mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
+    mpx_engine *e = eng;
+    const int W = e->W;
+    if (cap >= 0xFFFFFFF0ULL) return fail(eng, MPX_ERR_CAPACITY, "term capacity exceeds the 32-bit term index");
+    uint64_t *keys = nullptr;
+    double *coef = nullptr;
+    unsigned long long *table = nullptr;
+    const uint64_t tcap = next_pow2(std::max<uint64_t>(2 * cap, 64));
+    const uint64_t q_cap = cap + static_cast<uint64_t>(e->grid) * kBlock;
+    Scratch nsc = e->sc;
+    cudaError_t ce = cudaSuccess;
+    auto A = [&](void **p, size_t bytes) {
+        if (ce == cudaSuccess) ce = cudaMallocAsync(p, bytes, e->stream);
+    };
+    A(reinterpret_cast<void **>(&keys), cap * W * sizeof(uint64_t));
+    A(reinterpret_cast<void **>(&coef), cap * sizeof(double));
+    A(reinterpret_cast<void **>(&table), tcap * sizeof(unsigned long long));
+    A(reinterpret_cast<void **>(&nsc.q_src), q_cap * sizeof(uint32_t));
+    A(reinterpret_cast<void **>(&nsc.q_flag), q_cap * sizeof(uint8_t));
+    A(reinterpret_cast<void **>(&nsc.q_val), q_cap * sizeof(double));
+    A(reinterpret_cast<void **>(&nsc.emit_bits), (cap / 32 + 64) * sizeof(uint32_t));
+    A(reinterpret_cast<void **>(&nsc.aux), cap * sizeof(double));
+    if (ce != cudaSuccess) {
+        cudaFreeAsync(keys, e->stream);
+        cudaFreeAsync(coef, e->stream);
+        cudaFreeAsync(table, e->stream);
+        cudaGetLastError();
+        return fail(eng, MPX_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(ce));
+    }
+    if (n_keep > 0) {
+        MPX_CUDA(cudaMemcpyAsync(keys, e->st.keys, n_keep * W * sizeof(uint64_t), cudaMemcpyDeviceToDevice, e->stream));
+        MPX_CUDA(cudaMemcpyAsync(coef, e->st.coef, n_keep * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    }
+    cudaFreeAsync(e->st.keys, e->stream);
+    cudaFreeAsync(e->st.coef, e->stream);
+    cudaFreeAsync(e->st.table, e->stream);
+    cudaFreeAsync(e->sc.q_src, e->stream);
+    cudaFreeAsync(e->sc.q_flag, e->stream);
+    cudaFreeAsync(e->sc.q_val, e->stream);
+    cudaFreeAsync(e->sc.emit_bits, e->stream);
+    cudaFreeAsync(e->sc.aux, e->stream);
+    e->st.keys = keys;
+    e->st.coef = coef;
+    e->st.table = table;
+    e->st.cap = cap;
+    e->st.tmask = tcap - 1;
+    nsc.q_cap = q_cap;
+    e->sc = nsc;
+    MPX_CUDA(cudaMemsetAsync(table, 0xFF, tcap * sizeof(unsigned long long), e->stream));
+    pick_build(W)(e, 0, n_keep);
+    e->launches += n_keep > 0 ? 1 : 0;
+    MPX_CUDA(cudaGetLastError());
+    return MPX_OK;
+}
+
+mpx_status ensure_stats(mpx_engine *eng, uint64_t n) {
+    mpx_engine *e = eng;
+    if (n <= e->stats_cap) return MPX_OK;
+    cudaFreeAsync(e->d_stats, e->stream);
+    e->d_stats = nullptr;
+    const uint64_t c = std::max<uint64_t>(n, 1024);
+    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&e->d_stats), c * 4 * sizeof(uint64_t), e->stream));
+    e->stats_cap = c;
+    return MPX_OK;
+}
+
+void pair_swap_words(const uint64_t *g, uint64_t *out, int W) {
+    for (int w = 0; w < W; ++w) out[w] = ((g[w] & kEven) << 1) | ((g[w] >> 1) & kEven);
+}
+
+void interleave_words(const uint64_t *g, uint64_t *out, int W) {
+    int above = 0;
+    for (int w = 0; w < W; ++w) out[w] = 0;
+    for (int c = 64 * W - 1; c >= 0; --c) {
+        if (above & 1) out[c / 64] |= 1ULL << (c % 64);
+        above += static_cast<int>((g[c / 64] >> (c % 64)) & 1ULL);
+    }
+}
+
+void make_desc(const mpx_engine *e, const uint64_t *g, double angle, GateDesc &d) {
+    const int W = e->W;
+    std::memset(&d, 0, sizeof(d));
+    int gpop = 0, gy = 0;
+    for (int w = 0; w < W; ++w) {
+        d.g[w] = g[w];
+        gpop += __builtin_popcountll(g[w]);
+        const uint64_t v = g[w] & kEven, u = (g[w] >> 1) & kEven;
+        gy += __builtin_popcountll(v & ~u);
+    }
+    d.gpop = gpop;
+    d.gy = gy;
+    if (e->cfg.basis == MPX_BASIS_PAULI) {
+        pair_swap_words(g, d.fold, W);
+        d.g_odd = 0;
+    }
+    else {
+        for (int w = 0; w < W; ++w) d.fold[w] = g[w];
+        d.g_odd = gpop & 1;
+        interleave_words(g, d.wmask, W);
+    }
+    d.pivot_word = 0;
+    d.pivot_bit = 0;
+    for (int w = 0; w < W; ++w) {
+        if (g[w] != 0) {
+            d.pivot_word = w;
+            d.pivot_bit = g[w] & (~g[w] + 1);
+            break;
+        }
+    }
+    d.empty = gpop == 0;
+    // The same libm calls and argument as the reference (Engine.h:555-560, FusedApply.h:45-46).
+    const double c = std::cos(2.0 * angle);
+    const double s = std::sin(2.0 * angle);
+    d.cosv = c;
+    d.sinv = s;
+    d.abs_sin = std::fabs(s);
+    d.cos_zero = c == 0.0;
+    d.inv_cos = c != 0.0 ? 1.0 / c : 1.0;
+}
+
+mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const double *angles, uint64_t n,
+                          CircuitDev &cd) {
+    mpx_engine *e = eng;
+    std::vector<GateDesc> h(n);
+    for (uint64_t l = 0; l < n; ++l) make_desc(e, gen_words + l * e->W, angles[l], h[l]);
+    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&cd.d_desc), std::max<uint64_t>(n, 1) * sizeof(GateDesc),
+                             e->stream));
+    if (n > 0) {
+        MPX_CUDA(cudaMemcpyAsync(cd.d_desc, h.data(), n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));
+    }
+    MPX_CUDA(cudaStreamSynchronize(e->stream)); // h goes out of scope
+    cd.n = n;
+    cd.W = e->W;
+    cd.device = e->device;
+    cd.words.assign(gen_words, gen_words + n * e->W);
+    return MPX_OK;
+}
+
+// Applies the uploaded gates last to first (Heisenberg; MonomialPropagator.inl:720-733). Gates are
+// issued in chunks; the counters after chunk k are inspected while chunk k+1 already runs, so the GPU
+// is never idle on a healthy run. A stalled step makes the rest of the queue no-ops; the host waits,
+// grows the store and re-issues from that step.
+mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
+    mpx_engine *e = eng;
+    const uint64_t L = cd.n;
+    if (L == 0) return MPX_OK;
+    mpx_status s = ensure_stats(e, L);
+    if (s != MPX_OK) return s;
+    const GateFn gate = pick_gate(e->W, e->cfg.basis);
+    constexpr uint64_t kChunk = 48;
+    uint64_t step = 0;
+    uint64_t chunk_id = 0;
+    bool pending = false;
+    uint64_t pending_slot = 0;
+    for (;;) {
+        bool issued = false;
+        if (step < L) {
+            const uint64_t stop = std::min(L, step + kChunk);
+            for (uint64_t st = step; st < stop; ++st) {
+                gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
+            }
+            e->launches += 2 * (stop - step);
+            MPX_CUDA(cudaGetLastError());
+            const uint64_t slot = chunk_id & 1;
+            MPX_CUDA(cudaMemcpyAsync(&e->h_snap[slot], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+            MPX_CUDA(cudaEventRecord(e->ev[slot], e->stream));
+            step = stop;
+            issued = true;
+        }
+        if (pending) {
+            MPX_CUDA(cudaEventSynchronize(e->ev[pending_slot]));
+            const Counters snap = e->h_snap[pending_slot];
+            if (snap.stall != kNoStall) {
+                MPX_CUDA(cudaStreamSynchronize(e->stream));
+                const uint64_t at = snap.stall;
+                const uint64_t n = e->h_snap[pending_slot].n;
+                s = alloc_store(e, std::max<uint64_t>(4 * n, 2 * e->st.cap), n);
+                if (s != MPX_OK) return s;
+                Counters fresh{};
+                fresh.n = n;
+                fresh.n0 = n;
+                fresh.stall = kNoStall;
+                fresh.err = snap.err;
+                MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &fresh, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+                MPX_CUDA(cudaStreamSynchronize(e->stream));
+                step = at;
+                pending = false;
+                ++chunk_id;
+                continue;
+            }
+        }
+        if (!issued) break;
+        pending = true;
+        pending_slot = chunk_id & 1;
+        ++chunk_id;
+    }
+    MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    e->last_gates = L;
+    if (e->h_cnt->err != 0)
+        return fail(eng, MPX_ERR_STATE, "hash table probe limit reached (internal error); the store is invalid");
+    return MPX_OK;
+}
+
+mpx_status load_initial(mpx_engine *eng) {
+    mpx_engine *e = eng;
+    const int W = e->W;
+    if (e->n_init > 0) {
+        MPX_CUDA(cudaMemcpyAsync(e->st.keys, e->d_init_keys, e->n_init * W * sizeof(uint64_t),
+                                 cudaMemcpyDeviceToDevice, e->stream));
+        MPX_CUDA(cudaMemcpyAsync(e->st.coef, e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    }
+    MPX_CUDA(cudaMemsetAsync(e->st.table, 0xFF, (e->st.tmask + 1) * sizeof(unsigned long long), e->stream));
+    pick_build(W)(e, 0, e->n_init);
+    e->launches += e->n_init > 0 ? 1 : 0;
+    Counters c{};
+    c.n = e->n_init;
+    c.n0 = e->n_init;
+    c.stall = kNoStall;
+    c.err = 0;
+    MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    e->last_gates = 0;
+    return MPX_OK;
+}
+
+mpx_status validate_cfg(const mpx_config *c) {
+    if (c == nullptr) return fail(nullptr, MPX_ERR_INVALID, "config is NULL");
+    if (c->num_modes < 1 || c->num_modes > 256)
+        return fail(nullptr, MPX_ERR_INVALID, "logical_num_modes must be in the range [1, 256].");
+    if (c->basis != MPX_BASIS_PAULI && c->basis != MPX_BASIS_MAJORANA)
+        return fail(nullptr, MPX_ERR_INVALID, "basis must be 'majorana' or 'pauli'");
+    if (c->cutoff_type != MPX_CUTOFF_LENGTH && c->cutoff_type != MPX_CUTOFF_SUPPORT)
+        return fail(nullptr, MPX_ERR_INVALID, "cutoff_type must be 'length' or 'support'");
+    if (c->basis == MPX_BASIS_PAULI && c->cutoff_type != MPX_CUTOFF_SUPPORT)
+        return fail(nullptr, MPX_ERR_INVALID,
+                    "Pauli basis requires cutoff_type == Support (Length has no Pauli-weight meaning under the "
+                    "Pauli encoding).");
+    if (c->has_lower_atol && c->has_upper_atol && c->upper_atol < c->lower_atol)
+        return fail(nullptr, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
+    return MPX_OK;
+}
+
+}  // namespace
+
+// ----- C ABI ------------------------------------------------------------------------------------------------
+
+extern "C" {
+
+mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef, uint64_t n_obs,
+                      double core, const uint64_t *state_mask, mpx_engine **out) {
+    if (out == nullptr) return fail(nullptr, MPX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    mpx_status s = validate_cfg(cfg);
+    if (s != MPX_OK) return s;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, MPX_ERR_NO_DEVICE, "no CUDA device is visible; the engine has no CPU fallback");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, MPX_ERR_INVALID, "device ordinal out of range");
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return fail(nullptr, MPX_ERR_NO_DEVICE, "the engine is built for sm_100a (B200) only");
+    }
+    auto *e = new (std::nothrow) mpx_engine();
+    if (e == nullptr) return fail(nullptr, MPX_ERR_NOMEM, "host allocation failed");
+    e->cfg = *cfg;
+    e->W = ((cfg->num_modes + 31) / 32);
+    e->tr.cutoff_type = cfg->cutoff_type;
+    e->tr.cutoff = cfg->cutoff;
+    e->tr.has_lower = cfg->has_lower_atol;
+    e->tr.lower = cfg->lower_atol;
+    e->tr.has_upper = cfg->has_upper_atol;
+    e->tr.upper = cfg->upper_atol;
+    e->device = cfg->device;
+    e->core = core;
+    for (int w = 0; w < e->W; ++w) e->mask.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
+    e->grid = std::min(prop.multiProcessorCount * 8, kMaxGrid);
+    mpx_engine *eng = e;
+    auto bail = [&](mpx_status st) {
+        g_create_error = e->err;
+        mpx_destroy(e);
+        return st;
+    };
+    if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        e->err = "cannot create a CUDA stream";
+        return bail(MPX_ERR_CUDA);
+    }
+    cudaError_t ce = cudaMalloc(reinterpret_cast<void **>(&e->d_cnt), sizeof(Counters));
+    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_cnt), sizeof(Counters));
+    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.q_count), e->grid * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_anti), e->grid * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_out), sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_out), sizeof(double));
+    if (ce == cudaSuccess && n_obs > 0) {
+        ce = cudaMalloc(reinterpret_cast<void **>(&e->d_init_keys), n_obs * e->W * sizeof(uint64_t));
+        if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_init_coef), n_obs * sizeof(double));
+        if (ce == cudaSuccess)
+            ce = cudaMemcpy(e->d_init_keys, obs_words, n_obs * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(e->d_init_coef, obs_coef, n_obs * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    if (ce != cudaSuccess) {
+        e->err = std::string("CUDA setup failed: ") + cudaGetErrorString(ce);
+        cudaGetLastError();
+        return bail(MPX_ERR_CUDA);
+    }
+    e->n_init = n_obs;
+    const uint64_t cap = std::max<uint64_t>({cfg->capacity_hint, 4 * n_obs, 4096});
+    s = alloc_store(eng, cap, 0);
+    if (s != MPX_OK) return bail(s);
+    s = load_initial(eng);
+    if (s != MPX_OK) return bail(s);
+    *out = e;
+    return MPX_OK;
+}
+
+mpx_status mpx_propagate(mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n_layers) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    mpx_engine *eng = e;
+    if (n_layers > 0 && (gen_words == nullptr || angles == nullptr))
+        return fail(eng, MPX_ERR_INVALID, "gen_words/angles are NULL");
+    MPX_CUDA(cudaSetDevice(e->device));
+    CircuitDev cd;
+    mpx_status s = upload_circuit(e, gen_words, angles, n_layers, cd);
+    if (s == MPX_OK) s = run_circuit(e, cd);
+    cudaFreeAsync(cd.d_desc, e->stream);
+    cudaStreamSynchronize(e->stream);
+    cd.d_desc = nullptr;
+    return s;
+}
+
+mpx_status mpx_circuit_upload(mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n_layers,
+                              mpx_circuit **out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    *out = nullptr;
+    if (n_layers > 0 && (gen_words == nullptr || angles == nullptr))
+        return fail(eng, MPX_ERR_INVALID, "gen_words/angles are NULL");
+    MPX_CUDA(cudaSetDevice(e->device));
+    auto *c = new (std::nothrow) mpx_circuit();
+    if (c == nullptr) return fail(eng, MPX_ERR_NOMEM, "host allocation failed");
+    mpx_status s = upload_circuit(e, gen_words, angles, n_layers, *c);
+    if (s != MPX_OK) {
+        mpx_circuit_destroy(c);
+        return s;
+    }
+    *out = c;
+    return MPX_OK;
+}
+
+mpx_status mpx_circuit_set_angles(mpx_engine *e, mpx_circuit *c, const double *angles) {
+    if (e == nullptr || c == nullptr || (c->n > 0 && angles == nullptr)) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    std::vector<GateDesc> h(c->n);
+    for (uint64_t l = 0; l < c->n; ++l) make_desc(e, c->words.data() + l * e->W, angles[l], h[l]);
+    MPX_CUDA(cudaSetDevice(e->device));
+    if (c->n > 0) {
+        MPX_CUDA(cudaMemcpyAsync(c->d_desc, h.data(), c->n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    return MPX_OK;
+}
+
+mpx_status mpx_propagate_circuit(mpx_engine *e, const mpx_circuit *c) {
+    if (e == nullptr || c == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    MPX_CUDA(cudaSetDevice(e->device));
+    return run_circuit(e, *c);
+}
+
+void mpx_circuit_destroy(mpx_circuit *c) {
+    if (c == nullptr) return;
+    if (c->d_desc != nullptr) {
+        cudaSetDevice(c->device);
+        cudaFree(c->d_desc);
+    }
+    delete c;
+}
+
+mpx_status mpx_expectation(mpx_engine *e, double *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    MPX_CUDA(cudaSetDevice(e->device));
+    pick_exp(e->W, e->cfg.basis)(e);
+    k_expect_final<<<1, 32, 0, e->stream>>>(e->d_partial, static_cast<uint32_t>(e->grid), e->core, e->d_out);
+    e->launches += 2;
+    MPX_CUDA(cudaGetLastError());
+    MPX_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    *out = *e->h_out;
+    return MPX_OK;
+}
+
+mpx_status mpx_size(mpx_engine *e, uint64_t *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    MPX_CUDA(cudaSetDevice(e->device));
+    MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    *out = e->h_cnt->n;
+    return MPX_OK;
+}
+
+mpx_status mpx_words(mpx_engine *e, uint32_t *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    *out = static_cast<uint32_t>(e->W);
+    return MPX_OK;
+}
+
+mpx_status mpx_export(mpx_engine *e, uint64_t *words, double *coefs, uint64_t cap, uint64_t *n_out) {
+    if (e == nullptr || n_out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    uint64_t n = 0;
+    mpx_status s = mpx_size(e, &n);
+    if (s != MPX_OK) return s;
+    *n_out = n;
+    const uint64_t k = std::min(n, cap);
+    if (k > 0) {
+        if (words != nullptr)
+            MPX_CUDA(cudaMemcpyAsync(words, e->st.keys, k * e->W * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+        if (coefs != nullptr)
+            MPX_CUDA(cudaMemcpyAsync(coefs, e->st.coef, k * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    return MPX_OK;
+}
+
+mpx_status mpx_gate_stats(mpx_engine *e, uint64_t *out4, uint64_t max_gates, uint64_t *n_out) {
+    if (e == nullptr || n_out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    const uint64_t L = e->last_gates;
+    *n_out = L;
+    if (L == 0 || out4 == nullptr) return MPX_OK;
+    std::vector<uint64_t> h(4 * L);
+    MPX_CUDA(cudaMemcpyAsync(h.data(), e->d_stats, 4 * L * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+    uint64_t n_final = 0;
+    mpx_status s = mpx_size(e, &n_final);
+    if (s != MPX_OK) return s;
+    for (uint64_t g = 0; g < L; ++g) {
+        const uint64_t next = g + 1 < L ? h[4 * (g + 1)] : n_final;
+        h[4 * g + 3] = next - h[4 * g];
+    }
+    const uint64_t k = std::min(L, max_gates);
+    std::memcpy(out4, h.data(), 4 * k * sizeof(uint64_t));
+    return MPX_OK;
+}
+
+mpx_status mpx_reset(mpx_engine *e) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    mpx_engine *eng = e;
+    MPX_CUDA(cudaSetDevice(e->device));
+    return load_initial(e);
+}
+
+mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    e->cfg.cutoff = cutoff;
+    e->tr.cutoff = cutoff;
+    return MPX_OK;
+}
+
+mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    if (has_value && e->tr.has_upper && e->tr.upper < value)
+        return fail(e, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
+    e->cfg.has_lower_atol = has_value;
+    e->cfg.lower_atol = value;
+    e->tr.has_lower = has_value;
+    e->tr.lower = value;
+    return MPX_OK;
+}
+
+mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    if (has_value && e->tr.has_lower && value < e->tr.lower)
+        return fail(e, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
+    e->cfg.has_upper_atol = has_value;
+    e->cfg.upper_atol = value;
+    e->tr.has_upper = has_value;
+    e->tr.upper = value;
+    return MPX_OK;
+}
+
+mpx_status mpx_device_view(mpx_engine *e, const uint64_t **keys, double **coefs, uint64_t *n) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    if (keys) *keys = e->st.keys;
+    if (coefs) *coefs = e->st.coef;
+    if (n) return mpx_size(e, n);
+    return MPX_OK;
+}
+
+mpx_status mpx_stream(mpx_engine *e, void **stream) {
+    if (e == nullptr || stream == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    *stream = e->stream;
+    return MPX_OK;
+}
+
+mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    *out = e->launches;
+    return MPX_OK;
+}
+
+const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }
+
+void mpx_destroy(mpx_engine *e) {
+    if (e == nullptr) return;
+    if (e->stream != nullptr) {
+        cudaSetDevice(e->device);
+        cudaStreamSynchronize(e->stream);
+    }
+    free_store(e);
+    cudaFree(e->d_cnt);
+    cudaFreeHost(e->h_cnt);
+    cudaFreeHost(e->h_snap);
+    for (auto &ev : e->ev)
+        if (ev != nullptr) cudaEventDestroy(ev);
+    cudaFree(e->sc.q_count);
+    cudaFree(e->sc.blk_anti);
+    cudaFree(e->d_partial);
+    cudaFree(e->d_out);
+    cudaFreeHost(e->h_out);
+    cudaFree(e->d_init_keys);
+    cudaFree(e->d_init_coef);
+    cudaFree(e->d_stats);
+    if (e->stream != nullptr) cudaStreamDestroy(e->stream);
+    cudaGetLastError();
+    delete e;
+}
+
+}  // extern "C"
