@@ -1,0 +1,327 @@
+"""Benchmark of the Heisenberg propagation hot path on B200: term-gate updates per second.
+
+Workload (one "step"): the 10x10 kicked-Ising circuit (100 qubits, 20 layers of RZZ on the 180 lattice
+edges then RX on the 100 sites = 5600 gates, angles U[0, 0.3 pi) from seed 1234), observable
+(1/100) sum_i Z_i, Pauli weight <= 10, lower_atol 1e-5, FP64, propagated in full from the initial
+observable. A term-gate update is one term present in the store when one gate is applied; the rate is
+sum_g n_g / time.
+
+* ``value``: device time (CUDA events on the engine's stream) of ``mpx_propagate_circuit`` with the circuit
+  and the initial store already resident in HBM; the store is reset (untimed) before every step and L2 is
+  flushed (a 256 MiB write) between steps.
+* ``e2e``: the same rate through the public C ABI with host buffers, per step: ``mpx_create`` from the host
+  observable, ``mpx_propagate`` from the host circuit arrays (host-to-device copy inside), ``mpx_expectation``
+  (device-to-host read of <O>), ``mpx_destroy``.
+* ``roofline``: the sweep kernel (the per-gate pass over every stored key). Algorithmic bytes per launch
+  ``8W n_g + 16 a_g`` (read every key once, read+write every anticommuting coefficient) over its
+  event-timed duration, against the measured HBM copy bandwidth.
+* ``cpu_baseline``: the unmodified reference engine (compiled from its own sources into
+  ``oracle/_ref/libmpref.so``) propagating the same circuit on the host cores.
+
+``--impl reference`` times that reference engine alone on the same workload and prints its own line.
+Multi-GPU (``--gpus N`` under torchrun): N independent replicas of the workload, one per GPU (the
+single-operator path has no partitioned form yet); value = all ranks' updates / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _peaks() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import datetime
+
+    import torch.distributed as dist
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    return rank, ws, local, dist
+
+
+def _cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_reference(wl, steps: int, warmup: int, partitions: int) -> dict:
+    """The unmodified reference engine on the host cores: per step, one full propagate of ``wl``."""
+    import oracle
+
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libmpref.so is missing (build it with oracle/build_ref.sh)")
+    # Warm-up: a 400-gate prefix per warm-up step (pages the library and allocator in; CPU code has no JIT).
+    for _ in range(warmup):
+        eng = oracle.RefEngine(wl, partitions=partitions)
+        eng.propagate(n_layers=min(400, wl.n_layers))
+        eng.close()
+    secs, updates = [], None
+    for _ in range(steps):
+        eng = oracle.RefEngine(wl, partitions=partitions)
+        secs.append(eng.propagate())
+        eng.close()
+    return {"seconds": secs}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mpx", choices=["mpx", "reference"])
+    ap.add_argument("--workload", default="ising100", choices=["ising100", "line20", "hubbard6x6"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-partitions", type=int, default=0, help="reference partitions (0: all host threads)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    from monoprop_b200 import workloads as WL
+
+    wl = WL.BY_NAME[args.workload]()
+    rank, world, local, dist = _dist()
+    cores = args.cpu_partitions or _cpu_threads()
+    config = {"workload": f"{wl.name}: {wl.num_modes} modes, {wl.n_layers} gates, {wl.basis}, cutoff {wl.cutoff}, "
+                          f"lower_atol {wl.lower_atol}", "n_gates": wl.n_layers, "words": wl.words,
+              "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # Sum of n_g for the workload, from the oracle port's counters (identical to the reference's).
+        t = time_reference(wl, args.steps, args.warmup, cores)
+        updates = _updates(wl)
+        secs = t["seconds"]
+        v = updates * len(secs) / sum(secs)
+        line = {"metric": "term-gate updates/s", "value": v, "unit": "updates/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded circuit)", "config": config, "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "reference",
+                                 "sample": f"full {wl.name} propagate per step, partitions={cores}"},
+                "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    from monoprop_b200 import _native
+
+    torch.cuda.set_device(local)
+    if dist is not None:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    gw = wl.gen_words()
+    ang = wl.angles()
+    keys, coefs, core = wl.encoded_observable()
+
+    eng = _native.engine_for(wl, device=local)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
+    circ = eng.upload(gw, ang)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def one_step(profile: bool):
+        eng.reset()
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        eng.set_profiling(profile)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.propagate_circuit(circ)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    for _ in range(args.warmup):
+        one_step(False)
+    stats = eng.gate_stats()
+    updates = stats.term_gate_updates
+    n, anti, app = stats.n.astype(np.float64), stats.anti.astype(np.float64), stats.appended.astype(np.float64)
+    W = wl.words
+    sweep_bytes = float((8 * W * n + 16 * anti).sum())
+    path_bytes = float((8 * W * n + 16 * anti + (8 * W + 8) * app).sum())
+
+    launches0 = eng.launch_count()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, sweep_ms, resolve_ms = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            ms.append(one_step(True))
+            s_ms, r_ms, _ = eng.kernel_times()
+            sweep_ms.append(s_ms)
+            resolve_ms.append(r_ms)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = eng.launch_count() - launches0
+    total_ms = sum(ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = updates * world / (ms_per_step * 1e-3)
+    ev_dev = eng.expectation()
+
+    # End to end through the C ABI with host buffers (create + propagate + expectation + destroy).
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2 = _native.engine_for(wl, device=local)
+        e2.propagate(gw, ang)
+        ev2 = e2.expectation()
+        e2.close()
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_total = sum(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = updates * world / (e2e_total / args.steps * 1e-3)
+    h2d = int(gw.nbytes + ang.nbytes + keys.nbytes + coefs.nbytes)
+
+    peak, peak_kind = _peaks()
+    sweep_avg_s = statistics.mean(sweep_ms) * 1e-3
+    achieved = sweep_bytes / sweep_avg_s / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_sweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic": None, "algorithmic_bytes_per_launch": sweep_bytes / wl.n_layers,
+                "avg_launch_us": sweep_avg_s / wl.n_layers * 1e6,
+                "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms)},
+                "path_bytes_per_step": path_bytes,
+                "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
+    traffic_file = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            roofline["traffic"] = json.load(f).get("k_sweep_bytes_per_launch")
+
+    if dist is not None:
+        dist.barrier()
+    if rank != 0:
+        eng.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.ref_available():
+            secs = time_reference(wl, 1, 0, cores)["seconds"]
+            cpu = {"value": updates / secs[0], "unit": "updates/s", "cores": cores, "kind": "reference",
+                   "sample": f"one full {wl.name} propagate (all {wl.n_layers} gates), partitions={cores}",
+                   "seconds": secs[0]}
+        else:
+            cpu = {"value": None, "unit": "updates/s", "cores": 0, "kind": "reference",
+                   "sample": "oracle/_ref/libmpref.so not built"}
+
+    line = {"metric": "term-gate updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuit)",
+            "config": config, "term_gate_updates_per_step": updates, "final_terms": int(stats.n[-1] + stats.appended[-1]),
+            "expectation": ev_dev, "expectation_e2e": ev2,
+            "e2e": {"value": e2e, "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8,
+                    "ms_per_step": e2e_total / args.steps},
+            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _updates(wl) -> int:
+    """sum_g n_g of ``wl`` from the oracle port's per-gate counters (equal to the engine's)."""
+    import oracle
+
+    r = oracle.run_port(wl)
+    return int(r.counts[:, 0].sum())
+
+
+if __name__ == "__main__":
+    main()

@@ -125,6 +125,13 @@ MPX_API mpx_status mpx_stream(mpx_engine *e, void **stream);
 /* Number of engine kernel launches issued since the engine was created. */
 MPX_API mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out);
 
+/* Per-kernel timing. With profiling on, every sweep and resolve launch of a propagate call is bracketed
+ * by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms) for the
+ * last propagate call. The reference has no device kernels; this replaces nothing there (its closest
+ * counterpart is the per-layer wall time the bench harness records, benches/bench_models.py). */
+MPX_API mpx_status mpx_set_profiling(mpx_engine *e, int32_t on);
+MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, uint64_t *n_gates);
+
 MPX_API const char *mpx_last_error(const mpx_engine *e);
 MPX_API void mpx_destroy(mpx_engine *e);
 

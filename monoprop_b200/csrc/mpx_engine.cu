@@ -62,6 +62,12 @@ struct mpx_engine {
     double *d_out = nullptr;
     double *h_out = nullptr; // pinned
     uint64_t launches = 0;
+    // Per-kernel event timing (mpx_set_profiling): start/stop events around every sweep and resolve
+    // launch of the last propagate call, summed on the host afterwards.
+    int profile = 0;
+    std::vector<cudaEvent_t> pev;
+    double t_sweep_ms = 0.0, t_resolve_ms = 0.0;
+    uint64_t n_sweep = 0, n_resolve = 0;
     std::string err;
 };
 
@@ -91,8 +97,13 @@ uint64_t next_pow2(uint64_t x) {
 
 template <int W, int B>
 void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
+    cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
+    if (ev) cudaEventRecord(ev[0], e->stream);
     k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr);
+    if (ev) cudaEventRecord(ev[1], e->stream);
+    if (ev) cudaEventRecord(ev[2], e->stream);
     k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats);
+    if (ev) cudaEventRecord(ev[3], e->stream);
 }
 
 template <int W, int B>
@@ -325,6 +336,13 @@ mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
     if (L == 0) return MPX_OK;
     mpx_status s = ensure_stats(e, L);
     if (s != MPX_OK) return s;
+    if (e->profile) {
+        while (e->pev.size() < 4 * L) {
+            cudaEvent_t ev = nullptr;
+            MPX_CUDA(cudaEventCreate(&ev));
+            e->pev.push_back(ev);
+        }
+    }
     const GateFn gate = pick_gate(e->W, e->cfg.basis);
     constexpr uint64_t kChunk = 48;
     uint64_t step = 0;
@@ -376,6 +394,17 @@ mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
     MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     e->last_gates = L;
+    if (e->profile) {
+        e->t_sweep_ms = e->t_resolve_ms = 0.0;
+        for (uint64_t st = 0; st < L; ++st) {
+            float a = 0.f, b = 0.f;
+            MPX_CUDA(cudaEventElapsedTime(&a, e->pev[4 * st], e->pev[4 * st + 1]));
+            MPX_CUDA(cudaEventElapsedTime(&b, e->pev[4 * st + 2], e->pev[4 * st + 3]));
+            e->t_sweep_ms += a;
+            e->t_resolve_ms += b;
+        }
+        e->n_sweep = e->n_resolve = L;
+    }
     if (e->h_cnt->err != 0)
         return fail(eng, MPX_ERR_STATE, "hash table probe limit reached (internal error); the store is invalid");
     return MPX_OK;
@@ -689,6 +718,21 @@ mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out) {
     return MPX_OK;
 }
 
+mpx_status mpx_set_profiling(mpx_engine *e, int32_t on) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    e->profile = on != 0;
+    return MPX_OK;
+}
+
+mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, uint64_t *n_gates) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    if (!e->profile) return fail(e, MPX_ERR_STATE, "profiling is off (mpx_set_profiling)");
+    if (sweep_ms) *sweep_ms = e->t_sweep_ms;
+    if (resolve_ms) *resolve_ms = e->t_resolve_ms;
+    if (n_gates) *n_gates = e->n_sweep;
+    return MPX_OK;
+}
+
 const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }
 
 void mpx_destroy(mpx_engine *e) {
@@ -703,6 +747,7 @@ void mpx_destroy(mpx_engine *e) {
     cudaFreeHost(e->h_snap);
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
+    for (auto &ev : e->pev) cudaEventDestroy(ev);
     cudaFree(e->sc.q_count);
     cudaFree(e->sc.blk_anti);
     cudaFree(e->d_partial);
