@@ -148,7 +148,14 @@ def main() -> None:
     ap.add_argument("--workload", default="ising100", choices=["ising100", "line20", "hubbard6x6"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-partitions", type=int, default=0, help="reference partitions (0: all host threads)")
+    ap.add_argument("--kernel-case", type=int, default=0,
+                    help="profiling case instead of the benchmark: a store of this many random 100-qubit terms of "
+                         "Pauli weight <= 10, then the last --case-gates gates of the 10x10 circuit")
+    ap.add_argument("--case-gates", type=int, default=4)
     args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args.kernel_case, args.case_gates)
+        return
     if args.warmup < 3:
         args.warmup = 3
 
@@ -313,6 +320,35 @@ def main() -> None:
     eng.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def kernel_case(n_terms: int, n_gates: int) -> None:
+    """A large store built in one upload (few launches before the profiled ones), then a few gates."""
+    from monoprop_b200 import _native
+    from monoprop_b200 import workloads as WL
+
+    wl = WL.ising100()
+    rng = np.random.default_rng(5)
+    tier, W = 128, 4
+    keys = np.zeros((n_terms, W), dtype=np.uint64)
+    qubits = rng.integers(0, 100, size=(n_terms, 10))
+    kinds = rng.integers(1, 4, size=(n_terms, 10))  # 1: X (slot 2q), 2: Y (2q+1), 3: Z (both)
+    for j in range(10):
+        for slot_off, sel in ((0, kinds[:, j] != 2), (1, kinds[:, j] != 1)):
+            bit = (2 * tier - 1) - (2 * qubits[:, j] + slot_off)
+            word, pos = bit // 64, (bit % 64).astype(np.uint64)
+            for w in range(W):
+                m = sel & (word == w)
+                keys[m, w] |= np.uint64(1) << pos[m]
+    keys = np.unique(keys, axis=0)
+    coefs = rng.uniform(-1e-2, 1e-2, size=keys.shape[0])
+    eng = _native.Engine(basis="pauli", cutoff_type="support", cutoff=wl.cutoff, num_modes=100, keys=keys,
+                         coefs=coefs, core=0.0, state_mask=wl.state_mask(), lower_atol=wl.lower_atol)
+    eng.propagate(wl.gen_words()[-n_gates:], wl.angles()[-n_gates:])
+    st = eng.gate_stats()
+    print(json.dumps({"kernel_case_terms": int(keys.shape[0]), "n_g": st.n.tolist(), "a_g": st.anti.tolist(),
+                      "e_g": st.emitted.tolist(), "m_g": st.appended.tolist()}), flush=True)
+    eng.close()
 
 
 def _updates(wl) -> int:

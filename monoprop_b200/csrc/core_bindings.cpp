@@ -1,0 +1,352 @@
+// core_bindings.cpp -- the `_core` Python module: per-tier engine classes MonomialPropagator032 ...
+// MonomialPropagator256 with the reference's constructor keywords, method names and error types
+// (src/monoprop/bindings/binder.h:54-274, bindings.cpp.in:98-134), implemented in C++ over the engine's C
+// ABI (include/mpx.h). This host layer does what the reference's C++ facade does around the per-gate
+// kernel: validation before mutation, observable encoding (MonomialPropagator.inl:73-188), parameter
+// binding angle_l = theta[map_l] * g_l (MPFunctions.cpp:57-69) and the decoded, filtered, 1e-12-rounded
+// export of evolved_operator (MonomialPropagator.inl:1099-1127).
+//
+// Scope: the Heisenberg propagate path. schrodinger_cutoff, basis_change, a stored graph (build_graph,
+// graph functionals, contract_partially with a graph) and MPI communicators raise NotImplementedError.
+#include <pybind11/complex.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <complex>
+#include <cstdint>
+#include <map>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mpx.h"
+
+namespace py = pybind11;
+
+namespace {
+
+using OperatorDict = std::map<std::vector<size_t>, std::complex<double>>;
+
+// Reference error classes (MonomialPropagator.h:59-68, MonomialPropagator.inl:46-71): invalid_argument
+// subclasses surface as ValueError, runtime_error subclasses as RuntimeError.
+struct CutoffConfigError : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+struct PropagatorConfigError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct GraphStateConflict : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct NotSupported : std::logic_error {
+    using std::logic_error::logic_error;
+};
+
+int cutoff_type_code(const std::string &s) {
+    if (s == "length") return MPX_CUTOFF_LENGTH;
+    if (s == "support") return MPX_CUTOFF_SUPPORT;
+    throw std::invalid_argument("Invalid cutoff_type '" + s + "'. Valid options are: 'length', 'support'");
+}
+
+int basis_code(const std::string &s) {
+    if (s == "majorana") return MPX_BASIS_MAJORANA;
+    if (s == "pauli") return MPX_BASIS_PAULI;
+    throw std::invalid_argument("Invalid basis '" + s + "'. Valid options are: 'majorana', 'pauli'");
+}
+
+// i^k for k = C(w, 2) mod 4: the Hermitian phase of a weight-w Majorana monomial.
+std::complex<double> hermitian_phase(size_t w) {
+    switch ((w * (w - 1) / 2) % 4) {
+    case 0: return {1.0, 0.0};
+    case 1: return {0.0, 1.0};
+    case 2: return {-1.0, 0.0};
+    default: return {0.0, -1.0};
+    }
+}
+
+template <size_t Tier>
+class Propagator {
+public:
+    static constexpr size_t kWords = Tier / 32;
+
+    Propagator(const OperatorDict &initial_operator, unsigned int cutoff, const std::vector<size_t> &initial_state,
+               py::object comm, std::optional<unsigned int> schrodinger_cutoff, std::optional<double> lower_atol,
+               std::optional<double> upper_atol, const std::string &cutoff_type,
+               std::optional<std::vector<std::vector<size_t>>> basis_change, size_t logical_num_modes,
+               const std::string &basis, size_t /*partitions*/)
+        : logical_(logical_num_modes), state_(initial_state) {
+        if (!comm.is_none()) throw NotSupported("comm: the B200 engine runs on one GPU and takes no communicator");
+        if (schrodinger_cutoff.has_value())
+            throw NotSupported("schrodinger_cutoff: the B200 engine implements the Heisenberg picture");
+        if (logical_ == 0 || logical_ > Tier)
+            throw PropagatorConfigError("logical_num_modes (" + std::to_string(logical_) + ") must be in the range [1, " +
+                                        std::to_string(Tier) + "].");
+        cfg_.basis = basis_code(basis);
+        cfg_.cutoff_type = cutoff_type_code(cutoff_type);
+        if (cfg_.basis == MPX_BASIS_PAULI && cfg_.cutoff_type != MPX_CUTOFF_SUPPORT)
+            throw CutoffConfigError("Pauli basis requires cutoff_type == Support (Length has no Pauli-weight meaning "
+                                    "under the Pauli encoding).");
+        if (basis_change.has_value()) {
+            if (cfg_.basis == MPX_BASIS_PAULI)
+                throw CutoffConfigError("Pauli basis does not support basis_change.");
+            throw NotSupported("basis_change: not implemented by the B200 engine");
+        }
+        if (upper_atol && lower_atol && *upper_atol < *lower_atol)
+            throw PropagatorConfigError("upper_atol (" + std::to_string(*upper_atol) +
+                                        ") must be greater than or equal to lower_atol (" +
+                                        std::to_string(*lower_atol) + ").");
+        cfg_.cutoff = cutoff;
+        cfg_.has_lower_atol = lower_atol.has_value();
+        cfg_.lower_atol = lower_atol.value_or(0.0);
+        cfg_.has_upper_atol = upper_atol.has_value();
+        cfg_.upper_atol = upper_atol.value_or(0.0);
+        // The engine sizes keys by the storage tier of num_modes; pass the tier so W = Tier/32 and keys
+        // compare word for word with the reference's Monomial<Tier>.
+        cfg_.num_modes = static_cast<int32_t>(Tier);
+        cfg_.device = 0;
+        cfg_.capacity_hint = 0;
+
+        std::vector<uint64_t> keys;
+        std::vector<double> coefs;
+        for (const auto &[indices, c] : initial_operator) {
+            std::vector<uint64_t> k(kWords, 0);
+            encode(indices, 2 * logical_, k.data());
+            const double enc = encode_coeff(indices.size(), c);
+            if (indices.empty()) {
+                core_ = enc;
+                continue;
+            }
+            keys.insert(keys.end(), k.begin(), k.end());
+            coefs.push_back(enc);
+        }
+        std::vector<uint64_t> mask(kWords, 0);
+        std::vector<size_t> occ;
+        for (size_t m : initial_state) {
+            if (m >= logical_)
+                throw std::invalid_argument("initial_state index " + std::to_string(m) + " is out of range; must be "
+                                            "less than " + std::to_string(logical_) + ".");
+            occ.push_back(2 * m);
+        }
+        encode(occ, 2 * Tier, mask.data());
+        check(mpx_create(&cfg_, keys.empty() ? nullptr : keys.data(), coefs.empty() ? nullptr : coefs.data(),
+                         coefs.size(), core_, mask.data(), &e_),
+              nullptr);
+    }
+
+    ~Propagator() { mpx_destroy(e_); }
+    Propagator(const Propagator &) = delete;
+    Propagator &operator=(const Propagator &) = delete;
+
+    // MonomialPropagator<N>::propagate (MonomialPropagator.h:121-125, .inl:692-718).
+    void propagate(const std::vector<std::vector<size_t>> &majoranas, const std::vector<size_t> &parameter_mapping,
+                   const std::vector<double> &gen_coeffs, const std::vector<double> &parameters,
+                   std::optional<unsigned int> only_rotate_len_k) {
+        const size_t L = majoranas.size();
+        if (parameter_mapping.size() != L || gen_coeffs.size() != L)
+            throw std::invalid_argument("majoranas (" + std::to_string(L) + "), parameter_mapping (" +
+                                        std::to_string(parameter_mapping.size()) + ") and gen_coeffs (" +
+                                        std::to_string(gen_coeffs.size()) + ") must have the same length.");
+        if (only_rotate_len_k.has_value()) throw NotSupported("only_rotate_len_k: not implemented by the B200 engine");
+        std::vector<uint64_t> words(L * kWords, 0);
+        std::vector<double> angles(L);
+        for (size_t l = 0; l < L; ++l) {
+            if (parameter_mapping[l] >= parameters.size())
+                throw std::invalid_argument("parameter_mapping[" + std::to_string(l) + "] = " +
+                                            std::to_string(parameter_mapping[l]) + " is out of range for " +
+                                            std::to_string(parameters.size()) + " parameters.");
+            encode(majoranas[l], 2 * logical_, words.data() + l * kWords);
+            angles[l] = parameters[parameter_mapping[l]] * gen_coeffs[l];
+        }
+        py::gil_scoped_release nogil;
+        check(mpx_propagate(e_, words.data(), angles.data(), L), e_);
+    }
+
+    // Graph-less expectation: e_core + sum over fully paired terms (MPFunctions.cpp:196-205).
+    double expectation_value(const std::vector<double> &parameters) {
+        if (!parameters.empty())
+            throw GraphStateConflict("expectation_value(parameters) needs a stored graph; after propagate() call it "
+                                     "with no parameters.");
+        double ev = 0.0;
+        check(mpx_expectation(e_, &ev), e_);
+        return ev;
+    }
+
+    std::pair<double, std::vector<double>> expectation_value_and_gradient(const std::vector<double> &parameters) {
+        return {expectation_value(parameters), {}};
+    }
+
+    // {indices: coefficient} of the evolved operator, |c| >= atol, decoded and rounded to 1e-12, with the
+    // core term added (binder.h:200-221, MonomialPropagator.inl:1099-1127).
+    py::dict evolved_operator(const std::vector<double> &parameters, double atol) {
+        if (!parameters.empty())
+            throw GraphStateConflict("evolved_operator(parameters) needs a stored graph; after propagate() call it "
+                                     "with no parameters.");
+        uint64_t n = 0;
+        check(mpx_size(e_, &n), e_);
+        std::vector<uint64_t> words(n * kWords);
+        std::vector<double> coefs(n);
+        uint64_t got = 0;
+        check(mpx_export(e_, words.data(), coefs.data(), n, &got), e_);
+        py::dict out;
+        for (uint64_t i = 0; i < n; ++i) {
+            if (std::abs(coefs[i]) < atol) continue;
+            std::vector<size_t> idx = decode(words.data() + i * kWords);
+            std::complex<double> c = cfg_.basis == MPX_BASIS_PAULI ? std::complex<double>(coefs[i], 0.0)
+                                                                   : coefs[i] * hermitian_phase(idx.size());
+            c = {std::round(c.real() * 1e12) / 1e12, std::round(c.imag() * 1e12) / 1e12};
+            py::list key;
+            for (size_t s : idx) key.append(s);
+            out[py::tuple(key)] = c;
+        }
+        if (std::abs(core_) >= atol) out[py::tuple()] = std::complex<double>(core_, 0.0);
+        return out;
+    }
+
+    size_t size() {
+        uint64_t n = 0;
+        check(mpx_size(e_, &n), e_);
+        return n;
+    }
+
+    unsigned int cutoff() const { return cfg_.cutoff; }
+    void set_cutoff(unsigned int c) {
+        check(mpx_set_cutoff(e_, c), e_);
+        cfg_.cutoff = c;
+    }
+    std::optional<double> lower_atol() const {
+        return cfg_.has_lower_atol ? std::optional<double>(cfg_.lower_atol) : std::nullopt;
+    }
+    void set_lower_atol(std::optional<double> v) {
+        check(mpx_set_lower_atol(e_, v.has_value(), v.value_or(0.0)), e_);
+        cfg_.has_lower_atol = v.has_value();
+        cfg_.lower_atol = v.value_or(0.0);
+    }
+    std::optional<double> upper_atol() const {
+        return cfg_.has_upper_atol ? std::optional<double>(cfg_.upper_atol) : std::nullopt;
+    }
+    void set_upper_atol(std::optional<double> v) {
+        check(mpx_set_upper_atol(e_, v.has_value(), v.value_or(0.0)), e_);
+        cfg_.has_upper_atol = v.has_value();
+        cfg_.upper_atol = v.value_or(0.0);
+    }
+    std::string cutoff_type() const { return cfg_.cutoff_type == MPX_CUTOFF_SUPPORT ? "support" : "length"; }
+    std::string basis() const { return cfg_.basis == MPX_BASIS_PAULI ? "pauli" : "majorana"; }
+    size_t num_modes() const { return logical_; }
+    double core_term() const { return core_; }
+    size_t operator_memory_bytes() { return size() * (8 * kWords + 8); }
+    uintptr_t engine_handle() const { return reinterpret_cast<uintptr_t>(e_); }
+
+private:
+    // MSb0 slot layout: slot s -> bit 2*Tier-1-s (AlgebraCommon.h:45-65); `limit` bounds the slot index.
+    static void encode(const std::vector<size_t> &slots, size_t limit, uint64_t *out) {
+        for (size_t s : slots) {
+            if (s >= limit)
+                throw std::invalid_argument("Majorana index " + std::to_string(s) +
+                                            " is out of range; must be less than " + std::to_string(limit) + ".");
+            const size_t b = 2 * Tier - 1 - s;
+            out[b / 64] ^= 1ULL << (b % 64);
+        }
+    }
+    static std::vector<size_t> decode(const uint64_t *k) {
+        std::vector<size_t> out;
+        for (size_t w = 0; w < kWords; ++w)
+            for (uint64_t x = k[w]; x != 0; x &= x - 1) out.push_back(2 * Tier - 1 - (64 * w + __builtin_ctzll(x)));
+        std::sort(out.begin(), out.end());
+        return out;
+    }
+    double encode_coeff(size_t weight, std::complex<double> c) const {
+        if (cfg_.basis == MPX_BASIS_PAULI) {
+            if (std::abs(c.imag()) > 1e-10) throw std::runtime_error("Non-real Pauli coeffs detected");
+            return c.real();
+        }
+        const std::complex<double> e = c / hermitian_phase(weight);
+        if (std::abs(e.imag()) > 1e-10) throw std::runtime_error("Non-Hermitian coeffs detected");
+        return e.real();
+    }
+    static void check(mpx_status s, const mpx_engine *e) {
+        if (s == MPX_OK) return;
+        const std::string msg = mpx_last_error(e);
+        if (s == MPX_ERR_INVALID) throw std::invalid_argument(msg);
+        throw std::runtime_error(msg);
+    }
+
+    mpx_config cfg_{};
+    size_t logical_;
+    std::vector<size_t> state_;
+    double core_ = 0.0;
+    mpx_engine *e_ = nullptr;
+};
+
+template <size_t Tier>
+void bind(py::module_ &m) {
+    using P = Propagator<Tier>;
+    char name[32];
+    std::snprintf(name, sizeof name, "MonomialPropagator%03zu", Tier);
+    py::class_<P>(m, name)
+        .def(py::init<const OperatorDict &, unsigned int, const std::vector<size_t> &, py::object,
+                      std::optional<unsigned int>, std::optional<double>, std::optional<double>, const std::string &,
+                      std::optional<std::vector<std::vector<size_t>>>, size_t, const std::string &, size_t>(),
+             py::arg("initial_operator"), py::arg("cutoff"), py::arg("initial_state"), py::arg("comm") = py::none(),
+             py::arg("schrodinger_cutoff") = py::none(), py::arg("lower_atol") = py::none(),
+             py::arg("upper_atol") = py::none(), py::arg("cutoff_type") = "length",
+             py::arg("basis_change") = py::none(), py::arg("logical_num_modes") = Tier, py::arg("basis") = "majorana",
+             py::arg("partitions") = 0)
+        .def("propagate", &P::propagate, py::arg("majoranas"), py::arg("parameter_mapping"), py::arg("gen_coeffs"),
+             py::arg("parameters"), py::arg("only_rotate_len_k") = py::none())
+        .def("expectation_value", &P::expectation_value, py::arg("parameters"))
+        .def("expectation_value_and_gradient", &P::expectation_value_and_gradient, py::arg("parameters"))
+        .def("evolved_operator", &P::evolved_operator, py::arg("parameters"), py::arg("atol"))
+        .def("size", &P::size)
+        .def("graph_size", [](P &) { return std::pair<size_t, size_t>(0, 0); })
+        .def("graph_layers", [](P &) { return size_t{0}; })
+        .def("n_gates", [](P &) { return size_t{0}; })
+        .def("operator_memory_bytes", &P::operator_memory_bytes)
+        .def("core_term", &P::core_term)
+        .def("_engine_handle", &P::engine_handle)
+        .def_property("cutoff", &P::cutoff, &P::set_cutoff)
+        .def_property("lower_atol", &P::lower_atol, &P::set_lower_atol)
+        .def_property("upper_atol", &P::upper_atol, &P::set_upper_atol)
+        .def_property_readonly("cutoff_type", &P::cutoff_type)
+        .def_property_readonly("basis", &P::basis)
+        .def_property_readonly("num_modes", &P::num_modes)
+        .def_property_readonly("schrodinger", [](P &) { return false; })
+        .def_property_readonly_static("storage_num_modes", [](py::object) { return Tier; });
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_core, m) {
+    m.doc() = "B200 propagation engine: per-tier MonomialPropagatorNNN classes over the mpx C ABI";
+    py::register_exception<NotSupported>(m, "NotSupportedError", PyExc_NotImplementedError);
+    py::register_exception<GraphStateConflict>(m, "GraphStateConflict", PyExc_RuntimeError);
+    py::register_exception<PropagatorConfigError>(m, "PropagatorConfigError", PyExc_RuntimeError);
+    py::register_exception<CutoffConfigError>(m, "CutoffConfigError", PyExc_ValueError);
+    bind<32>(m);
+    bind<64>(m);
+    bind<96>(m);
+    bind<128>(m);
+    bind<160>(m);
+    bind<192>(m);
+    bind<224>(m);
+    bind<256>(m);
+    // Module helpers of the reference (MajoranaAlgebra.h:45-51): a weight-w Majorana monomial is
+    // anti-Hermitian iff C(w,2) is odd; the generator correction is i^(C(w,2)+1).
+    m.def(
+        "is_antihermitian", [](const std::vector<size_t> &idx) { return ((idx.size() * (idx.size() - 1) / 2) & 1) != 0; },
+        py::arg("indices"));
+    m.def(
+        "antihermitian_generator_correction",
+        [](const std::vector<size_t> &idx) {
+            return hermitian_phase(idx.size()) * std::complex<double>(0.0, 1.0);
+        },
+        py::arg("indices"));
+    m.attr("MAX_NUM_MODES") = 256;
+    m.attr("has_mpi") = false;
+    m.attr("__build_type__") = "Release";
+    m.attr("__variant__") = "b200";
+    m.attr("__compiler_flags__") = "nvcc -gencode arch=compute_100a,code=sm_100a -O3";
+}
