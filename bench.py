@@ -282,10 +282,14 @@ def main() -> None:
                 "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms)},
                 "path_bytes_per_step": path_bytes,
                 "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
-    traffic_file = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
+    # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on the
+    # 8 M-term profiling case, see profiles/) scaled to this workload's algorithmic bytes per launch.
+    traffic_file = os.path.join(ROOT, "profiles", "k_sweep_traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
-            roofline["traffic"] = json.load(f).get("k_sweep_bytes_per_launch")
+            ratio = json.load(f)["traffic_over_algorithmic"]
+        roofline["traffic"] = ratio * sweep_bytes / wl.n_layers
+        roofline["traffic_source"] = "ncu ratio from profiles/k_sweep_traffic.json x algorithmic bytes"
 
     if dist is not None:
         dist.barrier()
