@@ -133,6 +133,23 @@ MPX_API mpx_status mpx_set_profiling(mpx_engine *e, int32_t on);
 MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, uint64_t *n_gates);
 
 MPX_API const char *mpx_last_error(const mpx_engine *e);
+
+/* <0|O|0> of a term store the caller holds in device memory, computed without allocating any device
+ * memory. It has no counterpart in the reference (whose store never leaves the host); it is for callers
+ * that cannot call cudaMalloc mid-run -- a host runtime that plans and owns all device memory and hands
+ * this library pre-sized buffers, or one that cannot afford the device-wide synchronisation that
+ * cudaMalloc/cudaFree imply. keys [n_terms][words] and coefs [n_terms] are device pointers in the layout
+ * mpx_device_view exposes; state_mask is a HOST array of `words` words; out is a device pointer to one
+ * double; stream is a cudaStream_t (NULL = legacy default stream); the call only enqueues work.
+ * The scratch is a fixed 32 KiB array compiled into the library, so n_terms is limited to
+ * 268435456 (larger stores return MPX_ERR_CAPACITY). The first call on each device does a one-time
+ * set-up: it looks the array up with cudaGetSymbolAddress, so that device must be current, and that first
+ * call should come before any stream capture on the device begins. Every call shares the one array: calls whose
+ * kernels may overlap on the GPU must be serialised by the caller. On failure a message is written to
+ * err (up to err_len bytes, NUL-terminated) when err is not NULL. */
+MPX_API mpx_status mpx_expectation_noalloc(int32_t basis, uint32_t words, const uint64_t *keys, const double *coefs,
+                                           uint64_t n_terms, const uint64_t *state_mask, double core, double *out,
+                                           void *stream, char *err, size_t err_len);
 MPX_API void mpx_destroy(mpx_engine *e);
 
 #ifdef __cplusplus
