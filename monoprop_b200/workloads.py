@@ -192,3 +192,24 @@ def batch_ising50(n_instances: int = 256, seed: int = 99, min_depth: int = 4, ma
 
 
 BY_NAME = {"line20": line20, "ising100": ising100, "hubbard6x6": hubbard6x6}
+
+
+def from_circuit(name: str, operator, circuit, *, cutoff: int, cutoff_type: str = "length",
+                 lower_atol: float | None = None, upper_atol: float | None = None) -> Workload:
+    """Workload of a front-end circuit and observable (``PauliOperator`` or ``MajoranaOperator``).
+
+    The gate expansion is :func:`monoprop_b200.circuit.expand_monomials` (the reference's
+    ``expand_monomials``); a ``PauliOperator`` observable is taken in the native Pauli slot encoding.
+    """
+    from .circuit import expand_monomials
+    from .operators import PauliOperator
+
+    if isinstance(operator, PauliOperator):
+        basis, terms, n = "pauli", operator.get_local_operator().terms, operator.num_qubits
+    else:
+        basis, terms, n = "majorana", operator.get_majorana_operator().terms, operator.num_modes
+    monos, g, pmap, _ = expand_monomials(circuit.gates, circuit.resolved_mapping, n)
+    params = np.asarray(circuit.parameters, dtype=np.float64)
+    return Workload(name, basis, n, [tuple(m) for m in monos], np.asarray(g, dtype=np.float64),
+                    np.asarray(pmap, dtype=np.int64), params, dict(terms), list(circuit.initial_state), cutoff,
+                    cutoff_type, lower_atol, upper_atol)

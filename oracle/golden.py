@@ -1,0 +1,80 @@
+"""Loading the golden fixtures of ``tests/golden/`` (test infrastructure, like the rest of ``oracle``)."""
+
+from __future__ import annotations
+
+import hashlib
+import os
+
+import numpy as np
+
+from monoprop_b200.encoding import canonical_order, words_to_slots
+from monoprop_b200.workloads import Workload
+
+GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden")
+
+SEEDED = ["line20", "line20_L200", "hubbard6x6_L400", "ising100_L600", "ising50_d2", "ising50_d3", "ising100_L1200"]
+REF_CASES = [f"ref_{c}{t}" for c in ("rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact")
+             for t in ("", "_atol1e-10")]
+
+
+def load(name: str) -> dict:
+    with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def fixture_workload(g: dict, name: str = "fixture") -> Workload:
+    """Majorana workload stored in a ``ref_*`` fixture (engine arrays, infinite cutoff)."""
+    n = int(g["num_modes"])
+    off, flat = g["gate_slots_off"], g["gate_slots_flat"]
+    slots = [tuple(int(s) for s in flat[off[i]:off[i + 1]]) for i in range(len(off) - 1)]
+    obs = {}
+    for k, c in zip(g["obs_keys"], g["obs_coefs"]):
+        mono = words_to_slots(k, n)
+        w = len(mono)
+        obs[mono] = complex(c) * (1j) ** ((w * (w - 1) // 2) % 4)  # decode back to the operator's coefficient
+    if float(g["core"]) != 0.0:
+        obs[()] = complex(float(g["core"]))
+    la = float(g["lower_atol"])
+    return Workload(name, "majorana", n, slots, g["gen_coeffs"], g["param_map"], g["params"], obs,
+                    [int(i) for i in g["initial_state"]], int(g["cutoff"]), "length", None if np.isnan(la) else la)
+
+
+def check_against(g: dict, keys: np.ndarray, coefs: np.ndarray, ev: float, rtol: float = 1e-10) -> None:
+    """Asserts that (keys, coefs, ev) equal the golden result: keys bit-exact, coefficients and <O> within rtol."""
+    order = canonical_order(keys)
+    k, c = np.ascontiguousarray(keys[order]), coefs[order]
+    assert k.shape[0] == int(g["n"]), (k.shape[0], int(g["n"]))
+    assert hashlib.sha256(k.tobytes()).hexdigest() == g["sha256"].item().decode(), "monomial set differs"
+    if "keys" in g:
+        assert np.array_equal(k, g["keys"])
+        tol = rtol * np.maximum(np.abs(c), np.abs(g["coefs"])) + 1e-15
+        assert np.all(np.abs(c - g["coefs"]) <= tol), float(np.max(np.abs(c - g["coefs"])))
+    else:
+        assert abs(c.sum() - float(g["coef_sum"])) <= rtol * max(1.0, float(np.abs(c).sum()))
+        assert abs((c * c).sum() - float(g["coef_sumsq"])) <= rtol * max(1.0, float((c * c).sum()))
+    e = float(g["expectation"])
+    assert abs(ev - e) <= rtol * max(1.0, abs(e)), (ev, e)
+
+
+def random_workload(seed: int, basis: str) -> Workload:
+    """Random circuit on few modes with truncation active (small cutoffs, both atols)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(3, 7))
+    L = int(rng.integers(10, 60))
+    slots = []
+    for _ in range(L):
+        w = int(rng.integers(1, 5))
+        slots.append(tuple(sorted(rng.choice(2 * n, size=w, replace=False).tolist())))
+    g = rng.choice([-1.0, -0.5, 0.5, 1.0], size=L)
+    params = rng.uniform(-np.pi, np.pi, size=L)
+    j = int(rng.integers(0, L))
+    params[j] = np.pi / 4 / abs(g[j])  # cos(2 angle) ~ 6e-17: the partner value stored/cos is ill-conditioned
+    obs = {tuple(sorted(rng.choice(2 * n, size=2, replace=False).tolist())): 1.0 + 0j for _ in range(3)}
+    if basis == "pauli":
+        return Workload(f"rand_pauli_{seed}", "pauli", n, slots, g, np.arange(L), params,
+                          {k: complex(abs(v)) for k, v in obs.items()}, [0] if n > 1 else [], int(rng.integers(1, 3)),
+                          "support", float(rng.choice([1e-3, 1e-2])), float(rng.choice([0.05, 0.2])))
+    obs = {k: (1j if len(k) % 4 in (2, 3) else 1.0) for k in obs}
+    return Workload(f"rand_maj_{seed}", "majorana", n, slots, g, np.arange(L), params, obs,
+                      list(range(0, n, 2)), int(rng.integers(2, 5)), str(rng.choice(["length", "support"])),
+                      float(rng.choice([1e-3, 1e-2])), float(rng.choice([0.05, 0.2])))

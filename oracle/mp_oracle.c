@@ -223,7 +223,9 @@ static int phase_of(const mpo_state *s, const gate_ctx *c, const uint64_t *m, co
     for (int w = 0; w < W; ++w) par ^= popc(m[w] & c->wmask[w]) & 1;
     static const int REAL[4] = {1, 0, -1, 0};
     int ppop = mpop + c->gpop - 2 * ov;
-    int power = (nc2(mpop) + nc2(c->gpop) - nc2(ppop) + 3) % 4;
+    /* reduced into [0, 4): the reference evaluates this in unsigned arithmetic, where a negative
+     * intermediate wraps by 2^64, a multiple of 4 */
+    int power = (((nc2(mpop) + nc2(c->gpop) - nc2(ppop) + 3) % 4) + 4) % 4;
     return (par ? -1 : 1) * REAL[power];
 }
 

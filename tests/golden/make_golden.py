@@ -1,0 +1,111 @@
+"""Generates the golden fixtures in this directory from the UNMODIFIED reference engine.
+
+Run in a container that has the reference sources (the GPU hosts do not): it builds
+``oracle/_ref/libmpref.so`` from them (``oracle/build_ref.sh``) and writes
+
+* ``<workload>.npz`` -- seeded workloads propagated by the reference engine (``partitions=1``), raw FP64
+  coefficients exported at the C++ level (not the rounded ``evolved_operator`` dict), keys sorted
+  canonically, ``<0|O|0>``; bigger stores keep only a digest: term count, SHA-256 of the sorted keys,
+  sum and sum of squares of the coefficients in key order;
+* ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
+  (``tests/data/{rx_rz_ry_rz_exact,random_exact,lih_fermionic_spin_exact}.msgpack``), re-expressed as
+  engine arrays by this repository's front-end (``Circuit.from_dense_arrays`` + ``expand_monomials``,
+  ``MajoranaOperator`` canonicalisation), with the fixture's exact energy and gradient and the reference
+  engine's raw output at infinite cutoff (``cutoff = 2 n``).
+
+Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT]``.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from monoprop_b200 import workloads as W  # noqa: E402
+from monoprop_b200.circuit import Circuit  # noqa: E402
+from monoprop_b200.encoding import canonical_order  # noqa: E402
+from monoprop_b200.operators import MajoranaOperator  # noqa: E402
+
+FULL_LIMIT = 40_000  # stores up to this many terms are stored in full
+
+SEEDED = [
+    ("line20", W.line20, None),
+    ("line20_L200", W.line20, 200),
+    ("hubbard6x6_L400", W.hubbard6x6, 400),
+    ("ising100_L600", W.ising100, 600),
+    ("ising50_d2", lambda: W.ising50(2), None),
+    ("ising50_d3", lambda: W.ising50(3), None),
+    ("ising100_L1200", W.ising100, 1200),
+]
+
+REF_CASES = ["rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact"]
+
+
+def digest(keys: np.ndarray, coefs: np.ndarray) -> dict:
+    order = canonical_order(keys)
+    k, c = np.ascontiguousarray(keys[order]), coefs[order]
+    return {"n": np.int64(k.shape[0]), "sha256": np.bytes_(hashlib.sha256(k.tobytes()).hexdigest()),
+            "coef_sum": np.float64(c.sum()), "coef_sumsq": np.float64((c * c).sum())}
+
+
+def save_result(path: str, keys: np.ndarray, coefs: np.ndarray, ev: float, extra: dict) -> None:
+    order = canonical_order(keys)
+    payload = {"expectation": np.float64(ev), **digest(keys, coefs), **extra}
+    if keys.shape[0] <= FULL_LIMIT:
+        payload["keys"] = np.ascontiguousarray(keys[order])
+        payload["coefs"] = coefs[order]
+    np.savez_compressed(path, **payload)
+
+
+def fixture_workload(name: str, reference_root: str, lower_atol=None):
+    import msgpack
+
+    with open(os.path.join(reference_root, "tests", "data", name + ".msgpack"), "rb") as f:
+        d = msgpack.unpackb(f.read())
+    n = int(d["num_modes"])
+    circ = Circuit.from_dense_arrays([tuple(m) for m in d["majoranas"]], d["gen_coeffs"], d["param_inds"], n,
+                                     d["parameters"], d["hartree_fock"])
+    ham = d["hamiltonian"]
+    op = MajoranaOperator({tuple(k): complex(r, i) for k, r, i in zip(ham["keys"], ham["real"], ham["imag"])}, n)
+    wl = W.from_circuit(name, op, circ, cutoff=2 * n, cutoff_type="length", lower_atol=lower_atol)
+    return wl, float(d["actual_energy"]), np.asarray(d["actual_gradient"], dtype=np.float64)
+
+
+def main(reference_root: str = "/root/reference") -> None:
+    oracle.build(reference_root)
+    if not oracle.ref_available():
+        raise SystemExit("reference oracle could not be built")
+    for name, make, L in SEEDED:
+        wl = make()
+        r = oracle.run_ref(wl, n_layers=L)
+        save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
+                    {"n_layers": np.int64(wl.n_layers if L is None else L)})
+        print(name, r.keys.shape[0], r.expectation)
+    for case in REF_CASES:
+        for tag, la in (("", None), ("_atol1e-10", 1e-10)):
+            wl, exact, grad = fixture_workload(case, reference_root, la)
+            r = oracle.run_ref(wl)
+            enc_keys, enc_coefs, core = wl.encoded_observable()
+            flat = np.asarray([s for m in wl.gate_slots for s in m], dtype=np.int64)
+            off = np.cumsum([0] + [len(m) for m in wl.gate_slots]).astype(np.int64)
+            save_result(os.path.join(HERE, f"ref_{case}{tag}.npz"), r.keys, r.coefs, r.expectation,
+                        {"exact_energy": np.float64(exact), "exact_gradient": grad,
+                         "num_modes": np.int64(wl.num_modes), "gate_slots_flat": flat, "gate_slots_off": off,
+                         "gen_coeffs": wl.gen_coeffs, "param_map": wl.param_map, "params": wl.params,
+                         "obs_keys": enc_keys, "obs_coefs": enc_coefs, "core": np.float64(core),
+                         "state_mask": wl.state_mask(), "initial_state": np.asarray(wl.initial_state, np.int64),
+                         "cutoff": np.int64(wl.cutoff),
+                         "lower_atol": np.float64(np.nan if la is None else la)})
+            print(case + tag, r.keys.shape[0], r.expectation, exact)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

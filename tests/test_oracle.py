@@ -1,0 +1,75 @@
+"""The oracle (C restatement in oracle/mp_oracle.c) pinned against the reference.
+
+* against the golden fixtures generated from the unmodified reference engine (tests/golden/), including
+  the reference's own exact-energy test fixtures at infinite cutoff (exact energy to 1e-12, the
+  reference tests' tolerance: tests/test_infinite_cutoff.py:39-68);
+* against the reference engine itself, live, when oracle/_ref/libmpref.so has been built here
+  (random Pauli and Majorana circuits exercising lower_atol, upper_atol rescue, odd-weight generators,
+  near-zero cosines and the fully-paired exemption);
+* on the analytic one-gate truncation cases of the reference's tests/test_coeff_trunc.py:59-96.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from monoprop_b200 import workloads as W
+from monoprop_b200.encoding import canonical_order
+from oracle import golden
+from oracle.golden import random_workload
+
+SEEDED = {"line20": (W.line20, None), "line20_L200": (W.line20, 200), "hubbard6x6_L400": (W.hubbard6x6, 400),
+          "ising100_L600": (W.ising100, 600), "ising50_d2": (lambda: W.ising50(2), None),
+          "ising50_d3": (lambda: W.ising50(3), None), "ising100_L1200": (W.ising100, 1200)}
+
+
+@pytest.mark.parametrize("name", golden.SEEDED)
+def test_port_matches_reference_golden(name):
+    make, L = SEEDED[name]
+    g = golden.load(name)
+    r = oracle.run_port(make(), n_layers=L)
+    golden.check_against(g, r.keys, r.coefs, r.expectation)
+
+
+@pytest.mark.parametrize("name", golden.REF_CASES)
+def test_port_reproduces_reference_fixture(name):
+    g = golden.load(name)
+    wl = golden.fixture_workload(g, name)
+    r = oracle.run_port(wl)
+    golden.check_against(g, r.keys, r.coefs, r.expectation)
+    if np.isnan(float(g["lower_atol"])):
+        assert abs(r.expectation - float(g["exact_energy"])) <= 1e-12
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built here")
+@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("basis", ["pauli", "majorana"])
+def test_port_matches_reference_live(seed, basis):
+    wl = random_workload(seed, basis)
+    a, b = oracle.run_port(wl), oracle.run_ref(wl)
+    ia, ib = canonical_order(a.keys), canonical_order(b.keys)
+    assert np.array_equal(a.keys[ia], b.keys[ib])
+    assert np.array_equal(a.coefs[ia], b.coefs[ib])
+    assert a.expectation == b.expectation
+
+
+def one_gate(cutoff, upper_atol, lower_atol):
+    """exp(i pi/6 m1 m2 m3 m4) on the observable i m0 m1 (tests/test_coeff_trunc.py:59-96)."""
+    return W.Workload("one_gate", "majorana", 5, [(1, 2, 3, 4)], np.array([1.0]), np.array([0]),
+                      np.array([np.pi / 6]), {(0, 1): 1j}, [], cutoff, "length", lower_atol, upper_atol)
+
+
+@pytest.mark.parametrize("cutoff, upper_atol, lower_atol, kept", [
+    (4, None, None, True), (1, 0.49, None, True), (1, 1.0, None, False), (4, None, 0.9, False),
+    (10, None, 0.1, True)])
+def test_analytic_one_gate_truncation(cutoff, upper_atol, lower_atol, kept):
+    r = oracle.run_port(one_gate(cutoff, upper_atol, lower_atol))
+    from monoprop_b200.encoding import words_to_slots
+    got = {words_to_slots(k, 5): c for k, c in zip(r.keys, r.coefs)}
+    # encoded coefficients: i m0 m1 -> 1 (÷ i^1); cos(pi/3) = 0.5; the sine branch m0 m2 m3 m4 carries
+    # -sin(pi/3) after decoding (i^C(4,2) = -1 encoding)
+    assert got[(0, 1)] == pytest.approx(0.5, abs=1e-15)
+    if kept:
+        assert got[(0, 2, 3, 4)] == pytest.approx(0.8660254037844386, abs=1e-15)
+    else:
+        assert (0, 2, 3, 4) not in got
