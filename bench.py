@@ -12,9 +12,13 @@ sum_g n_g / time.
 * ``e2e``: the same rate through the public C ABI with host buffers, per step: ``mpx_create`` from the host
   observable, ``mpx_propagate`` from the host circuit arrays (host-to-device copy inside), ``mpx_expectation``
   (device-to-host read of <O>), ``mpx_destroy``.
-* ``roofline``: the sweep kernel (the per-gate pass over every stored key). Algorithmic bytes per launch
-  ``8W n_g + 16 a_g`` (read every key once, read+write every anticommuting coefficient) over its
-  event-timed duration, against the measured HBM copy bandwidth.
+* ``roofline``: the sweep kernel (the per-gate anticommutation scan over every stored term). Its
+  algorithmic bytes per launch are what the bit-column scan must move: ``(f_g + 1) n_g / 8`` (the f_g
+  fold columns read, the leader-emitted bitmap written) ``+ 16 a_g`` (read+write of every anticommuting
+  coefficient) ``+ (8W + 13) e_g`` (key rows of the emitted terms, the query records written), over its
+  event-timed duration, against the measured HBM copy bandwidth. ``path_frac`` is the whole path against
+  the row-store formula ``sum_g 8W n_g + 16 a_g + (8W + 8) m_g`` over the device step time; the column
+  index lets the path move fewer bytes than that formula, so ``path_frac`` can exceed 1.
 * ``cpu_baseline``: the unmodified reference engine (compiled from its own sources into
   ``oracle/_ref/libmpref.so``) propagating the same circuit on the host cores.
 
@@ -152,6 +156,9 @@ def main() -> None:
                     help="profiling case instead of the benchmark: a store of this many random 100-qubit terms of "
                          "Pauli weight <= 10, then the last --case-gates gates of the 10x10 circuit")
     ap.add_argument("--case-gates", type=int, default=4)
+    ap.add_argument("--no-gradient", action="store_true", help="skip the <O> + full-gradient measurement")
+    ap.add_argument("--segment-layers", type=int, default=4,
+                    help="gradient checkpoint interval in circuit layers (the circuit repeats one layer of gates)")
     args = ap.parse_args()
     if args.kernel_case:
         kernel_case(args.kernel_case, args.case_gates)
@@ -224,21 +231,26 @@ def main() -> None:
     stats = eng.gate_stats()
     updates = stats.term_gate_updates
     n, anti, app = stats.n.astype(np.float64), stats.anti.astype(np.float64), stats.appended.astype(np.float64)
+    emitted = stats.emitted.astype(np.float64)
     W = wl.words
-    sweep_bytes = float((8 * W * n + 16 * anti).sum())
+    gpop = np.array([sum(bin(int(x)).count("1") for x in row) for row in gw], dtype=np.float64)
+    fold = gpop + ((gpop % 2 == 1) if wl.basis == "majorana" else 0)  # + the |M|-parity column
+    fold = fold[::-1]  # gates are applied last to first; stats are in application order
+    sweep_bytes = float(((fold + 1) * n / 8 + 16 * anti + (8 * W + 13) * emitted).sum())
     path_bytes = float((8 * W * n + 16 * anti + (8 * W + 8) * app).sum())
 
     launches0 = eng.launch_count()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    ms, sweep_ms, resolve_ms = [], [], []
+    ms, sweep_ms, resolve_ms, columns_ms = [], [], [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             ms.append(one_step(True))
-            s_ms, r_ms, _ = eng.kernel_times()
+            s_ms, r_ms, c_ms, _ = eng.kernel_times()
             sweep_ms.append(s_ms)
             resolve_ms.append(r_ms)
+            columns_ms.append(c_ms)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -251,6 +263,36 @@ def main() -> None:
     ms_per_step = total_ms / args.steps
     value = updates * world / (ms_per_step * 1e-3)
     ev_dev = eng.expectation()
+
+    # <O> + full gradient per second: forward with coefficient checkpoints every --segment-layers circuit
+    # layers, then the adjoint sweep (same engine, circuit resident), against the plain forward above.
+    grad_line = None
+    if not args.no_gradient:
+        seg = args.segment_layers * wl.extra.get("gates_per_layer", wl.n_layers)
+        eng.set_profiling(False)
+        g_ms = []
+        for i in range(1 + args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ev_g = eng.adjoint_forward(circ, seg)
+            grad = eng.adjoint_backward(circ)
+            b.record(stream)
+            b.synchronize()
+            if i > 0:
+                g_ms.append(a.elapsed_time(b))
+        g_total = sum(g_ms)
+        if dist is not None:
+            t = torch.tensor([g_total], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            g_total = float(t.item())
+        g_per = g_total / len(g_ms)
+        grad_line = {"metric": "<O>+full-gradient/s", "value": world * 1e3 / g_per, "unit": "gradients/s",
+                     "ms_per_eval": g_per, "forward_ms": ms_per_step, "cost_vs_forward": g_per / ms_per_step,
+                     "segment_gates": seg, "n_angles": int(wl.n_layers), "expectation": ev_g,
+                     "grad_abs_max": float(np.max(np.abs(grad)))}
 
     # End to end through the C ABI with host buffers (create + propagate + expectation + destroy).
     e2e_ms = []
@@ -279,7 +321,8 @@ def main() -> None:
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "traffic": None, "algorithmic_bytes_per_launch": sweep_bytes / wl.n_layers,
                 "avg_launch_us": sweep_avg_s / wl.n_layers * 1e6,
-                "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms)},
+                "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms),
+                                       "k_columns": statistics.mean(columns_ms)},
                 "path_bytes_per_step": path_bytes,
                 "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
     # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on the
@@ -319,7 +362,8 @@ def main() -> None:
             "expectation": ev_dev, "expectation_e2e": ev2,
             "e2e": {"value": e2e, "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8,
                     "ms_per_step": e2e_total / args.steps},
-            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary()}
+            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gradient": grad_line}
     print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

@@ -125,12 +125,26 @@ MPX_API mpx_status mpx_stream(mpx_engine *e, void **stream);
 /* Number of engine kernel launches issued since the engine was created. */
 MPX_API mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out);
 
-/* Per-kernel timing. With profiling on, every sweep and resolve launch of a propagate call is bracketed
- * by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms) for the
- * last propagate call. The reference has no device kernels; this replaces nothing there (its closest
- * counterpart is the per-layer wall time the bench harness records, benches/bench_models.py). */
+/* Gradient of <0|O|0> with respect to every gate angle (reverse mode over the frozen truncation structure
+ * of the forward pass). Replaces the reference's graph build + replayed gradient,
+ * MonomialPropagator<N>::build_graph (MonomialPropagator.inl:620-690) followed by
+ * expectation_value_and_gradient (MonomialPropagator.inl:1044-1050, MPFunctions.cpp:207-246).
+ * mpx_adjoint_forward resets the store to the initial operator, propagates circuit c saving the
+ * coefficient array every segment_gates gates (0 = one segment) and returns <0|O|0>; the engine then holds
+ * the evolved operator. mpx_adjoint_backward replays each segment from its checkpoint and returns
+ * grad_angles[l] = d<0|O|0>/d(angle_l) for every circuit layer l, angle_l = theta[map_l] * g_l (host
+ * buffer of c's n_layers doubles). Peak extra memory: the checkpoints plus, for the largest segment,
+ * 12 bytes per anticommuting term-gate pair and 25 bytes per emitted sine branch. */
+MPX_API mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation);
+MPX_API mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *grad_angles);
+
+/* Per-kernel timing. With profiling on, the sweep, resolve and column-append launches of every gate are
+ * bracketed by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms)
+ * for the last propagate call. The reference has no device kernels; this replaces nothing there (its
+ * closest counterpart is the per-layer wall time the bench harness records, benches/bench_models.py). */
 MPX_API mpx_status mpx_set_profiling(mpx_engine *e, int32_t on);
-MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, uint64_t *n_gates);
+MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, double *columns_ms,
+                                    uint64_t *n_gates);
 
 MPX_API const char *mpx_last_error(const mpx_engine *e);
 

@@ -22,7 +22,8 @@ _STATUS = {1: "MPX_ERR_INVALID", 2: "MPX_ERR_CUDA", 3: "MPX_ERR_NOMEM", 4: "MPX_
 EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_set_angles", "mpx_propagate_circuit",
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
-            "mpx_stream", "mpx_launch_count", "mpx_set_profiling", "mpx_kernel_times", "mpx_last_error",
+            "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_set_profiling", "mpx_kernel_times",
+            "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc")
 
 
@@ -76,8 +77,11 @@ def load() -> C.CDLL:
             "mpx_device_view": (st, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]),
             "mpx_stream": (st, [vp, C.POINTER(vp)]),
             "mpx_launch_count": (st, [vp, C.POINTER(u64)]),
+            "mpx_adjoint_forward": (st, [vp, vp, u64, C.POINTER(C.c_double)]),
+            "mpx_adjoint_backward": (st, [vp, vp, vp]),
             "mpx_set_profiling": (st, [vp, C.c_int32]),
-            "mpx_kernel_times": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(u64)]),
+            "mpx_kernel_times": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(u64)]),
             "mpx_last_error": (C.c_char_p, [vp]),
             "mpx_destroy": (None, [vp]),
             "mpx_expectation_noalloc": (st, [C.c_int32, C.c_uint32, vp, vp, u64, vp, C.c_double, vp, vp, C.c_char_p,
@@ -234,14 +238,26 @@ class Engine:
         self._check(self.lib.mpx_launch_count(self.h, C.byref(out)))
         return int(out.value)
 
+    def adjoint_forward(self, circuit: Circuit, segment_gates: int = 0) -> float:
+        """Reset, propagate ``circuit`` saving coefficient checkpoints every ``segment_gates`` gates; <O>."""
+        out = C.c_double(0.0)
+        self._check(self.lib.mpx_adjoint_forward(self.h, circuit.h, int(segment_gates), C.byref(out)))
+        return out.value
+
+    def adjoint_backward(self, circuit: Circuit) -> np.ndarray:
+        """d<O>/d(angle_l) for every layer l of ``circuit`` (after :meth:`adjoint_forward`)."""
+        out = np.zeros(max(circuit.n_layers, 1), dtype=np.float64)
+        self._check(self.lib.mpx_adjoint_backward(self.h, circuit.h, _p(out)))
+        return out[: circuit.n_layers]
+
     def set_profiling(self, on: bool) -> None:
         self._check(self.lib.mpx_set_profiling(self.h, int(bool(on))))
 
-    def kernel_times(self) -> tuple[float, float, int]:
-        """(summed sweep ms, summed resolve ms, gates) of the last propagate call (profiling on)."""
-        a, b, n = C.c_double(0.0), C.c_double(0.0), C.c_uint64(0)
-        self._check(self.lib.mpx_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(n)))
-        return a.value, b.value, int(n.value)
+    def kernel_times(self) -> tuple[float, float, float, int]:
+        """(summed sweep, resolve and column-append ms, gates) of the last propagate call (profiling on)."""
+        a, b, c, n = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0), C.c_uint64(0)
+        self._check(self.lib.mpx_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(n)))
+        return a.value, b.value, c.value, int(n.value)
 
     def close(self) -> None:
         if getattr(self, "h", None):

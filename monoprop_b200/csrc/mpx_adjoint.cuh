@@ -1,0 +1,155 @@
+// mpx_adjoint.cuh -- reverse-mode gradient of <0|O|0> with respect to every gate angle (sm_100a).
+//
+// The gradient is that of the frozen-structure surrogate the reference differentiates (ev_and_grad,
+// MPFunctions.cpp:207-246; state_operator_derivative_local, Evolution.cpp:439-469): every truncation
+// decision of the forward pass is kept, and each gate is the linear map A_g(angle) on the coefficient
+// vector
+//     anticommuting term i without a rotation partner:  c_i' = C c_i
+//     rotated pair (S emitter, T partner):             c_S' = C c_S - s phi c_T,  c_T' = C c_T + s phi c_S
+//     appended partner T (c_T = 0 before the gate):      c_S' = C c_S,               c_T' = s phi c_S
+// with C = cos(2 angle), s = sin(2 angle). With lambda the adjoint (dE/dc after the gate),
+//     dE/dangle_g = lambda'^T (dA_g/dangle) c_pre,   lambda_pre = A_g^T lambda'.
+//
+// Instead of inverting the forward maps (the reference un-scales by 1/cos, CosineRecompute.h:201-224),
+// the forward pass saves the coefficient array at segment boundaries; each segment is replayed from its
+// checkpoint with the forward kernels in replay mode, which log the pre-gate value of every
+// anticommuting term (undo log) and every rotated or appended pair with both pre-gate values (pair log).
+// The reverse sweep over that segment then needs no coefficients, no hash lookups and no division.
+#pragma once
+
+#include <cstdint>
+
+#include "mpx_device.cuh"
+
+namespace mpx {
+
+// Logs written by a replayed segment, indexed by the step's offsets (per-step bases are prefix sums of
+// the forward pass's a_g and e_g, so a step's records are contiguous).
+struct Tape {
+    uint32_t *u_idx; // undo log: anticommuting term index
+    double *u_val;   //           its coefficient before the gate
+    uint32_t *p_src; // pair log: emitter S
+    uint32_t *p_tgt; //           partner T
+    int8_t *p_code;  //           phase (+1 / -1 / 0) | 0x10 when T was appended by this gate
+    double *p_vs;    //           c_S before the gate
+    double *p_vt;    //           c_T before the gate (0 for an append)
+    const uint64_t *u_base; // [n_steps] first undo record of each step
+    const uint64_t *p_base; // [n_steps] first pair record of each step
+    unsigned long long *u_cnt; // [n_steps] undo records written per step
+    unsigned long long *p_cnt; // [n_steps] pair records written per step
+    const uint64_t *n_next;    // [n_steps] store size after each step (from the forward pass)
+};
+
+__device__ __forceinline__ double block_sum(double v, double *s_red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) t += s_red[w];
+    __syncthreads();
+    return t;
+}
+
+// After a replayed gate: the store size the forward pass reached after this step (appended partners
+// were looked up, not re-inserted).
+__global__ void k_replay_advance(Counters *__restrict__ cnt, const uint64_t *__restrict__ n_next, uint32_t step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && cnt->stall == kNoStall) cnt->n = n_next[step];
+}
+
+// lambda_i = d<0|O|0>/dc_i = state phase of a fully paired term, else 0 (MPOperator.h:235-254).
+template <int W, int BASIS>
+__global__ void __launch_bounds__(kBlock) k_adj_init(const uint64_t *__restrict__ keys, uint64_t n, StateMask sm,
+                                                      double *__restrict__ lam) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t m[W];
+        load_key<W>(keys, i, m);
+        uint64_t unpaired = 0;
+        int na = 0, pop = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            unpaired |= (m[w] & kEven) ^ ((m[w] >> 1) & kEven);
+            na += __popcll(m[w] & sm.w[w]);
+            pop += __popcll(m[w]);
+        }
+        double l = 0.0;
+        if (unpaired == 0) {
+            const int odd = BASIS == 1 ? (na & 1) : ((na + pop / 2) & 1);
+            l = odd ? -1.0 : 1.0;
+        }
+        lam[i] = l;
+    }
+}
+
+// Reverse step, part 1: the gate's rotated and appended pairs. Writes lambda of both endpoints, marks
+// them in `done` (the undo pass skips them) and adds their share of dE/dangle.
+__global__ void __launch_bounds__(kBlock) k_adj_pairs(Tape tp, const GateDesc *__restrict__ gates, uint32_t gate,
+                                                       uint32_t step, double *__restrict__ lam,
+                                                       uint32_t *__restrict__ done, double *__restrict__ grad) {
+    __shared__ double s_red[kBlock / 32];
+    const uint64_t base = tp.p_base[step];
+    const uint64_t cnt = tp.p_cnt[step];
+    if (cnt == 0) return;
+    const GateDesc &gd = gates[gate];
+    const double C = gd.cosv, S = gd.sinv;
+    double acc = 0.0;
+    for (uint64_t tb = blockIdx.x * static_cast<uint64_t>(kBlock); tb < cnt; tb += static_cast<uint64_t>(gridDim.x) * kBlock) {
+        const uint64_t k = tb + threadIdx.x;
+        if (k < cnt) {
+            const uint64_t r = base + k;
+            const uint32_t s = tp.p_src[r], t = tp.p_tgt[r];
+            const int8_t code = tp.p_code[r];
+            const bool appended = (code & 0x10) != 0;
+            const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
+            const double vs = tp.p_vs[r], vt = tp.p_vt[r];
+            const double ls = lam[s], lt = lam[t];
+            // d(c_S')/dangle = -2 s v_S - 2 C phi v_T;  d(c_T')/dangle = -2 s v_T + 2 C phi v_S
+            acc += ls * (-2.0 * S * vs - 2.0 * C * phi * vt) + lt * (-2.0 * S * vt + 2.0 * C * phi * vs);
+            lam[s] = C * ls + S * phi * lt;
+            atomicOr(&done[s >> 5], 1u << (s & 31));
+            if (!appended) {
+                lam[t] = C * lt - S * phi * ls;
+                atomicOr(&done[t >> 5], 1u << (t & 31));
+            }
+        }
+    }
+    const double t = block_sum(acc, s_red);
+    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&grad[gate], t);
+}
+
+// Reverse step, part 2: every anticommuting term of the gate. Terms not in a pair were only cos-scaled:
+// dE/dangle += lambda' (-2 s c_pre), lambda = C lambda'. Pair members were handled by part 1; their
+// done bit is cleared here (each appears once in the undo log), so `done` is all zero between gates.
+__global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__restrict__ gates, uint32_t gate,
+                                                      uint32_t step, double *__restrict__ lam,
+                                                      uint32_t *__restrict__ done, double *__restrict__ grad) {
+    __shared__ double s_red[kBlock / 32];
+    const uint64_t base = tp.u_base[step];
+    const uint64_t cnt = tp.u_cnt[step];
+    if (cnt == 0) return;
+    const GateDesc &gd = gates[gate];
+    const double C = gd.cosv, S = gd.sinv;
+    double acc = 0.0;
+    for (uint64_t tb = blockIdx.x * static_cast<uint64_t>(kBlock); tb < cnt; tb += static_cast<uint64_t>(gridDim.x) * kBlock) {
+        const uint64_t k = tb + threadIdx.x;
+        if (k < cnt) {
+            const uint64_t r = base + k;
+            const uint32_t i = tp.u_idx[r];
+            const uint32_t bit = 1u << (i & 31);
+            if (done[i >> 5] & bit) {
+                atomicAnd(&done[i >> 5], ~bit);
+            }
+            else {
+                const double l = lam[i];
+                acc += l * (-2.0 * S * tp.u_val[r]);
+                lam[i] = C * l;
+            }
+        }
+    }
+    const double t = block_sum(acc, s_red);
+    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&grad[gate], t);
+}
+
+}  // namespace mpx

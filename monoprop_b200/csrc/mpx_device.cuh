@@ -26,7 +26,8 @@ struct GateDesc {
     int32_t gpop, gy, g_odd, pivot_word;
     uint64_t pivot_bit;
     int32_t cos_zero, empty;
-    int32_t pad[2];
+    int32_t pivot_col; // physical bit index of the pivot: 64 * pivot_word + ctz(pivot_bit)
+    int32_t pad;
 };
 
 // Engine-wide truncation settings (CutoffContext.h:20-42, AlgebraCommon.h:229-243).
@@ -43,29 +44,37 @@ struct Counters {
     unsigned long long n0; // term count at the start of the current gate
     uint32_t stall;        // kNoStall, or the step index at which capacity ran out
     uint32_t err;          // nonzero: a bounded probe loop gave up (table inconsistent); results invalid
+    // Per-gate query and anticommuting-term counts, double-buffered by step parity: the sweep of step s
+    // accumulates into [s & 1] and clears [(s + 1) & 1] for the next gate.
+    unsigned long long q_total[2];
+    unsigned long long anti[2];
 };
 
 struct StateMask {
     uint64_t w[kMaxWords]; // slot 2m set for every occupied mode m of the reference state
 };
 
+// The key store is kept twice: as rows (keys, for the per-term work) and as bit-columns (cols, for the
+// anticommutation test). Column c (physical key bit c, c < 64W; c = 64W is the parity of |M|) is a
+// bitmap over terms: word j holds terms 32j .. 32j+31, bit (i & 31) for term i. The bits of a column
+// word beyond the live term count are zero.
 struct Store {
     uint64_t *keys;
     double *coef;
     unsigned long long *table;
-    uint64_t tmask; // table capacity - 1 (power of two)
-    uint64_t cap;   // term capacity
+    uint32_t *cols;   // [64W + 1][cstride]
+    uint64_t cstride; // 32-bit words per column
+    uint64_t tmask;   // table capacity - 1 (power of two)
+    uint64_t cap;     // term capacity
 };
 
 struct Scratch {
-    uint32_t *q_src;   // per-block query regions (block b owns [b*T, b*T + q_count[b]))
-    uint8_t *q_flag;   // bit0 follower, bits1-2 phase code (0:+1, 1:-1, 2:0)
-    double *q_val;     // pre-gate source coefficient v_src
-    uint32_t *q_count; // [grid]
-    uint32_t *blk_anti; // [grid]
-    uint32_t *emit_bits; // leader-emitted flags, one bit per term
-    double *aux;       // pre-gate coefficients, used only for cos == 0 gates
-    uint64_t q_cap;    // size of the query region arrays
+    uint32_t *q_src;     // emitted sine branches of the current gate, in any order
+    uint8_t *q_flag;     // bit0 follower, bits1-2 phase code (0:+1, 1:-1, 2:0)
+    double *q_val;       // pre-gate source coefficient v_src
+    uint32_t *emit_bits; // leader-emitted flags, one bit per term (column-word layout)
+    double *aux;         // pre-gate coefficients, used only for cos == 0 gates
+    uint64_t q_cap;      // size of the query arrays
 };
 
 __host__ __device__ inline uint64_t mix64(uint64_t x) {

@@ -36,6 +36,20 @@ struct mpx_circuit {
 };
 using CircuitDev = mpx_circuit;
 
+// Gradient state between mpx_adjoint_forward and mpx_adjoint_backward: coefficient checkpoints at
+// segment starts (keys are append-only, so a prefix of the final store plus its coefficients restores
+// any earlier state), the final coefficients, and the forward pass's per-gate counters.
+struct AdjointState {
+    const mpx_circuit *circuit = nullptr;
+    uint64_t L = 0;
+    std::vector<uint64_t> seg_lo; // first step of each segment
+    std::vector<uint64_t> ck_n;   // store size at each segment start
+    std::vector<double *> ck_coef;
+    double *final_coef = nullptr;
+    uint64_t n_final = 0;
+    std::vector<uint64_t> stats; // [L][4] n_g, a_g, e_g, (unused) per step
+};
+
 struct mpx_engine {
     mpx_config cfg{};
     int W = 1;
@@ -66,8 +80,9 @@ struct mpx_engine {
     // launch of the last propagate call, summed on the host afterwards.
     int profile = 0;
     std::vector<cudaEvent_t> pev;
-    double t_sweep_ms = 0.0, t_resolve_ms = 0.0;
-    uint64_t n_sweep = 0, n_resolve = 0;
+    double t_sweep_ms = 0.0, t_resolve_ms = 0.0, t_columns_ms = 0.0;
+    uint64_t n_sweep = 0;
+    AdjointState adj;
     std::string err;
 };
 
@@ -99,11 +114,27 @@ template <int W, int B>
 void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
     cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr);
+    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, Tape{});
     if (ev) cudaEventRecord(ev[1], e->stream);
+    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats, Tape{});
     if (ev) cudaEventRecord(ev[2], e->stream);
-    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats);
+    k_columns<W><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, 0, 0, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
+}
+
+// A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends.
+template <int W, int B>
+void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
+    k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
+    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
+                                                             tp);
+    k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
+}
+
+template <int W, int B>
+void launch_adj_init(mpx_engine *e, double *lam, uint64_t n) {
+    const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock + 1, static_cast<uint64_t>(e->grid) * 4);
+    k_adj_init<W, B><<<static_cast<unsigned>(blocks), kBlock, 0, e->stream>>>(e->st.keys, n, e->mask, lam);
 }
 
 template <int W, int B>
@@ -111,14 +142,20 @@ void launch_expect(mpx_engine *e) {
     k_expect<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, e->mask, e->d_partial);
 }
 
+// Hash table and bit-columns of terms [lo, hi).
 template <int W>
 void launch_build(mpx_engine *e, uint64_t lo, uint64_t hi) {
     if (hi <= lo) return;
     const uint64_t blocks = std::min<uint64_t>((hi - lo + 255) / 256, static_cast<uint64_t>(e->grid) * 4);
     k_build_table<W><<<static_cast<unsigned>(blocks), 256, 0, e->stream>>>(e->st, e->d_cnt, lo, hi);
+    const uint64_t cblocks = std::min<uint64_t>((hi - lo + 32 * kBlock - 1) / (32 * kBlock) + 1,
+                                                static_cast<uint64_t>(e->grid));
+    k_columns<W><<<static_cast<unsigned>(cblocks), kBlock, 0, e->stream>>>(e->st, e->d_cnt, lo, hi, 0);
 }
 
 using GateFn = void (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t);
+using ReplayFn = void (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t, const Tape &);
+using AdjInitFn = void (*)(mpx_engine *, double *, uint64_t);
 using ExpFn = void (*)(mpx_engine *);
 using BuildFn = void (*)(mpx_engine *, uint64_t, uint64_t);
 
@@ -129,6 +166,14 @@ GateFn gate_fn(int basis) {
 template <int W>
 ExpFn exp_fn(int basis) {
     return basis == 1 ? &launch_expect<W, 1> : &launch_expect<W, 0>;
+}
+template <int W>
+ReplayFn replay_fn(int basis) {
+    return basis == 1 ? &launch_replay<W, 1> : &launch_replay<W, 0>;
+}
+template <int W>
+AdjInitFn adj_init_fn(int basis) {
+    return basis == 1 ? &launch_adj_init<W, 1> : &launch_adj_init<W, 0>;
 }
 
 GateFn pick_gate(int W, int basis) {
@@ -155,6 +200,30 @@ ExpFn pick_exp(int W, int basis) {
     default: return exp_fn<8>(basis);
     }
 }
+ReplayFn pick_replay(int W, int basis) {
+    switch (W) {
+    case 1: return replay_fn<1>(basis);
+    case 2: return replay_fn<2>(basis);
+    case 3: return replay_fn<3>(basis);
+    case 4: return replay_fn<4>(basis);
+    case 5: return replay_fn<5>(basis);
+    case 6: return replay_fn<6>(basis);
+    case 7: return replay_fn<7>(basis);
+    default: return replay_fn<8>(basis);
+    }
+}
+AdjInitFn pick_adj_init(int W, int basis) {
+    switch (W) {
+    case 1: return adj_init_fn<1>(basis);
+    case 2: return adj_init_fn<2>(basis);
+    case 3: return adj_init_fn<3>(basis);
+    case 4: return adj_init_fn<4>(basis);
+    case 5: return adj_init_fn<5>(basis);
+    case 6: return adj_init_fn<6>(basis);
+    case 7: return adj_init_fn<7>(basis);
+    default: return adj_init_fn<8>(basis);
+    }
+}
 BuildFn pick_build(int W) {
     switch (W) {
     case 1: return &launch_build<1>;
@@ -174,6 +243,7 @@ void free_store(mpx_engine *e) {
     cudaFree(e->st.keys);
     cudaFree(e->st.coef);
     cudaFree(e->st.table);
+    cudaFree(e->st.cols);
     cudaFree(e->sc.q_src);
     cudaFree(e->sc.q_flag);
     cudaFree(e->sc.q_val);
@@ -195,8 +265,10 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     uint64_t *keys = nullptr;
     double *coef = nullptr;
     unsigned long long *table = nullptr;
+    uint32_t *cols = nullptr;
     const uint64_t tcap = next_pow2(std::max<uint64_t>(2 * cap, 64));
-    const uint64_t q_cap = cap + static_cast<uint64_t>(e->grid) * kBlock;
+    const uint64_t q_cap = cap;
+    const uint64_t cstride = ((cap + 31) / 32 + 31) / 32 * 32; // 128-byte aligned columns
     Scratch nsc = e->sc;
     cudaError_t ce = cudaSuccess;
     auto A = [&](void **p, size_t bytes) {
@@ -205,15 +277,22 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     A(reinterpret_cast<void **>(&keys), cap * W * sizeof(uint64_t));
     A(reinterpret_cast<void **>(&coef), cap * sizeof(double));
     A(reinterpret_cast<void **>(&table), tcap * sizeof(unsigned long long));
+    A(reinterpret_cast<void **>(&cols), (64 * W + 1) * cstride * sizeof(uint32_t));
     A(reinterpret_cast<void **>(&nsc.q_src), q_cap * sizeof(uint32_t));
     A(reinterpret_cast<void **>(&nsc.q_flag), q_cap * sizeof(uint8_t));
     A(reinterpret_cast<void **>(&nsc.q_val), q_cap * sizeof(double));
-    A(reinterpret_cast<void **>(&nsc.emit_bits), (cap / 32 + 64) * sizeof(uint32_t));
+    A(reinterpret_cast<void **>(&nsc.emit_bits), cstride * sizeof(uint32_t));
     A(reinterpret_cast<void **>(&nsc.aux), cap * sizeof(double));
     if (ce != cudaSuccess) {
         cudaFreeAsync(keys, e->stream);
         cudaFreeAsync(coef, e->stream);
         cudaFreeAsync(table, e->stream);
+        cudaFreeAsync(cols, e->stream);
+        cudaFreeAsync(nsc.q_src == e->sc.q_src ? nullptr : nsc.q_src, e->stream);
+        cudaFreeAsync(nsc.q_flag == e->sc.q_flag ? nullptr : nsc.q_flag, e->stream);
+        cudaFreeAsync(nsc.q_val == e->sc.q_val ? nullptr : nsc.q_val, e->stream);
+        cudaFreeAsync(nsc.emit_bits == e->sc.emit_bits ? nullptr : nsc.emit_bits, e->stream);
+        cudaFreeAsync(nsc.aux == e->sc.aux ? nullptr : nsc.aux, e->stream);
         cudaGetLastError();
         return fail(eng, MPX_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(ce));
     }
@@ -224,6 +303,7 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     cudaFreeAsync(e->st.keys, e->stream);
     cudaFreeAsync(e->st.coef, e->stream);
     cudaFreeAsync(e->st.table, e->stream);
+    cudaFreeAsync(e->st.cols, e->stream);
     cudaFreeAsync(e->sc.q_src, e->stream);
     cudaFreeAsync(e->sc.q_flag, e->stream);
     cudaFreeAsync(e->sc.q_val, e->stream);
@@ -232,13 +312,15 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     e->st.keys = keys;
     e->st.coef = coef;
     e->st.table = table;
+    e->st.cols = cols;
+    e->st.cstride = cstride;
     e->st.cap = cap;
     e->st.tmask = tcap - 1;
     nsc.q_cap = q_cap;
     e->sc = nsc;
     MPX_CUDA(cudaMemsetAsync(table, 0xFF, tcap * sizeof(unsigned long long), e->stream));
     pick_build(W)(e, 0, n_keep);
-    e->launches += n_keep > 0 ? 1 : 0;
+    e->launches += n_keep > 0 ? 2 : 0;
     MPX_CUDA(cudaGetLastError());
     return MPX_OK;
 }
@@ -294,6 +376,7 @@ void make_desc(const mpx_engine *e, const uint64_t *g, double angle, GateDesc &d
         if (g[w] != 0) {
             d.pivot_word = w;
             d.pivot_bit = g[w] & (~g[w] + 1);
+            d.pivot_col = 64 * w + __builtin_ctzll(g[w]);
             break;
         }
     }
@@ -330,7 +413,7 @@ mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const doub
 // issued in chunks; the counters after chunk k are inspected while chunk k+1 already runs, so the GPU
 // is never idle on a healthy run. A stalled step makes the rest of the queue no-ops; the host waits,
 // grows the store and re-issues from that step.
-mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
+mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_t hi) {
     mpx_engine *e = eng;
     const uint64_t L = cd.n;
     if (L == 0) return MPX_OK;
@@ -344,19 +427,21 @@ mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
         }
     }
     const GateFn gate = pick_gate(e->W, e->cfg.basis);
+    // Per-gate counters start from zero (the sweep of step s clears the other parity for step s+1).
+    MPX_CUDA(cudaMemsetAsync(&e->d_cnt->q_total, 0, sizeof(Counters::q_total) + sizeof(Counters::anti), e->stream));
     constexpr uint64_t kChunk = 48;
-    uint64_t step = 0;
+    uint64_t step = lo;
     uint64_t chunk_id = 0;
     bool pending = false;
     uint64_t pending_slot = 0;
     for (;;) {
         bool issued = false;
-        if (step < L) {
-            const uint64_t stop = std::min(L, step + kChunk);
+        if (step < hi) {
+            const uint64_t stop = std::min(hi, step + kChunk);
             for (uint64_t st = step; st < stop; ++st) {
                 gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
             }
-            e->launches += 2 * (stop - step);
+            e->launches += 3 * (stop - step);
             MPX_CUDA(cudaGetLastError());
             const uint64_t slot = chunk_id & 1;
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[slot], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
@@ -373,7 +458,7 @@ mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
                 const uint64_t n = e->h_snap[pending_slot].n;
                 s = alloc_store(e, std::max<uint64_t>(4 * n, 2 * e->st.cap), n);
                 if (s != MPX_OK) return s;
-                Counters fresh{};
+                Counters fresh{};  // per-gate counters restart at zero
                 fresh.n = n;
                 fresh.n0 = n;
                 fresh.stall = kNoStall;
@@ -395,19 +480,26 @@ mpx_status run_circuit(mpx_engine *eng, const CircuitDev &cd) {
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     e->last_gates = L;
     if (e->profile) {
-        e->t_sweep_ms = e->t_resolve_ms = 0.0;
-        for (uint64_t st = 0; st < L; ++st) {
-            float a = 0.f, b = 0.f;
+        e->t_sweep_ms = e->t_resolve_ms = e->t_columns_ms = 0.0;
+        for (uint64_t st = lo; st < hi; ++st) {
+            float a = 0.f, b = 0.f, c = 0.f;
             MPX_CUDA(cudaEventElapsedTime(&a, e->pev[4 * st], e->pev[4 * st + 1]));
-            MPX_CUDA(cudaEventElapsedTime(&b, e->pev[4 * st + 2], e->pev[4 * st + 3]));
+            MPX_CUDA(cudaEventElapsedTime(&b, e->pev[4 * st + 1], e->pev[4 * st + 2]));
+            MPX_CUDA(cudaEventElapsedTime(&c, e->pev[4 * st + 2], e->pev[4 * st + 3]));
             e->t_sweep_ms += a;
             e->t_resolve_ms += b;
+            e->t_columns_ms += c;
         }
-        e->n_sweep = e->n_resolve = L;
+        e->n_sweep = hi - lo;
     }
     if (e->h_cnt->err != 0)
         return fail(eng, MPX_ERR_STATE, "hash table probe limit reached (internal error); the store is invalid");
     return MPX_OK;
+}
+
+mpx_status run_circuit(mpx_engine *e, const CircuitDev &cd) {
+    e->adj.circuit = nullptr; // a plain propagation invalidates a pending gradient
+    return run_range(e, cd, 0, cd.n);
 }
 
 mpx_status load_initial(mpx_engine *eng) {
@@ -421,7 +513,7 @@ mpx_status load_initial(mpx_engine *eng) {
     }
     MPX_CUDA(cudaMemsetAsync(e->st.table, 0xFF, (e->st.tmask + 1) * sizeof(unsigned long long), e->stream));
     pick_build(W)(e, 0, e->n_init);
-    e->launches += e->n_init > 0 ? 1 : 0;
+    e->launches += e->n_init > 0 ? 2 : 0;
     Counters c{};
     c.n = e->n_init;
     c.n0 = e->n_init;
@@ -430,6 +522,175 @@ mpx_status load_initial(mpx_engine *eng) {
     MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     e->last_gates = 0;
+    return MPX_OK;
+}
+
+// ----- gradient (adjoint) -------------------------------------------------------------------------------
+
+void free_adjoint(mpx_engine *e) {
+    for (double *p : e->adj.ck_coef)
+        if (p != nullptr) cudaFreeAsync(p, e->stream);
+    if (e->adj.final_coef != nullptr) cudaFreeAsync(e->adj.final_coef, e->stream);
+    e->adj = AdjointState{};
+}
+
+// Forward pass for the gradient: resets the store to the initial operator, propagates the circuit
+// segment by segment (segment_gates gates each) and saves the coefficient array at every segment start
+// and at the end.
+mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+    mpx_engine *e = eng;
+    free_adjoint(e);
+    mpx_status s = load_initial(e);
+    if (s != MPX_OK) return s;
+    const uint64_t L = cd.n;
+    const uint64_t K = segment_gates == 0 ? std::max<uint64_t>(L, 1) : segment_gates;
+    uint64_t n = e->n_init;
+    for (uint64_t lo = 0; lo < L; lo += K) {
+        double *ck = nullptr;
+        MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double), e->stream));
+        e->adj.ck_coef.push_back(ck);
+        if (n > 0) MPX_CUDA(cudaMemcpyAsync(ck, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+        e->adj.seg_lo.push_back(lo);
+        e->adj.ck_n.push_back(n);
+        s = run_range(e, cd, lo, std::min(L, lo + K));
+        if (s != MPX_OK) {
+            free_adjoint(e);
+            return s;
+        }
+        n = e->h_cnt->n;
+    }
+    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(n, 1) * sizeof(double),
+                             e->stream));
+    if (n > 0)
+        MPX_CUDA(cudaMemcpyAsync(e->adj.final_coef, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    e->adj.n_final = n;
+    e->adj.L = L;
+    e->adj.stats.assign(4 * L, 0);
+    if (L > 0)
+        MPX_CUDA(cudaMemcpyAsync(e->adj.stats.data(), e->d_stats, 4 * L * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                 e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    e->last_gates = L;
+    e->adj.circuit = &cd;
+    return MPX_OK;
+}
+
+// Reverse sweep: per segment (last first) restore its checkpoint, replay it logging the tape, then walk
+// its gates backwards. grad_angles[l] = dE/d(angle_l) for circuit layer l (angle = theta[map] * g).
+mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_angles) {
+    mpx_engine *e = eng;
+    AdjointState &A = e->adj;
+    const uint64_t L = A.L;
+    const uint64_t nf = A.n_final;
+    const size_t S = A.seg_lo.size();
+    // per-step bases of the tape (prefix sums within each segment) and store sizes after each step
+    std::vector<uint64_t> u_base(L), p_base(L), n_next(L);
+    uint64_t u_max = 1, p_max = 1;
+    for (size_t sg = 0; sg < S; ++sg) {
+        const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
+        uint64_t u = 0, p = 0;
+        for (uint64_t st = lo; st < hi; ++st) {
+            u_base[st] = u;
+            p_base[st] = p;
+            u += A.stats[4 * st + 1];
+            p += A.stats[4 * st + 2];
+            n_next[st] = st + 1 < L ? A.stats[4 * (st + 1)] : nf;
+        }
+        u_max = std::max(u_max, u);
+        p_max = std::max(p_max, p);
+    }
+    Tape tp{};
+    uint64_t *d_steps = nullptr;  // u_base | p_base | n_next
+    unsigned long long *d_cnts = nullptr; // u_cnt | p_cnt
+    double *lam = nullptr, *grad = nullptr;
+    uint32_t *done = nullptr;
+    cudaError_t ce = cudaSuccess;
+    auto A_ = [&](void **ptr, size_t bytes) {
+        if (ce == cudaSuccess) ce = cudaMallocAsync(ptr, std::max<size_t>(bytes, 16), e->stream);
+    };
+    A_(reinterpret_cast<void **>(&tp.u_idx), u_max * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&tp.u_val), u_max * sizeof(double));
+    A_(reinterpret_cast<void **>(&tp.p_src), p_max * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&tp.p_tgt), p_max * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&tp.p_code), p_max * sizeof(int8_t));
+    A_(reinterpret_cast<void **>(&tp.p_vs), p_max * sizeof(double));
+    A_(reinterpret_cast<void **>(&tp.p_vt), p_max * sizeof(double));
+    A_(reinterpret_cast<void **>(&d_steps), 3 * L * sizeof(uint64_t));
+    A_(reinterpret_cast<void **>(&d_cnts), 2 * L * sizeof(unsigned long long));
+    A_(reinterpret_cast<void **>(&lam), nf * sizeof(double));
+    A_(reinterpret_cast<void **>(&grad), L * sizeof(double));
+    A_(reinterpret_cast<void **>(&done), ((nf + 31) / 32) * sizeof(uint32_t));
+    auto release = [&]() {
+        for (void *ptr : {static_cast<void *>(tp.u_idx), static_cast<void *>(tp.u_val), static_cast<void *>(tp.p_src),
+                          static_cast<void *>(tp.p_tgt), static_cast<void *>(tp.p_code), static_cast<void *>(tp.p_vs),
+                          static_cast<void *>(tp.p_vt), static_cast<void *>(d_steps), static_cast<void *>(d_cnts),
+                          static_cast<void *>(lam), static_cast<void *>(grad), static_cast<void *>(done)})
+            if (ptr != nullptr) cudaFreeAsync(ptr, e->stream);
+    };
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return fail(eng, MPX_ERR_NOMEM, std::string("gradient tape allocation failed (use shorter segments): ") +
+                                            cudaGetErrorString(ce));
+    }
+    tp.u_base = d_steps;
+    tp.p_base = d_steps + L;
+    tp.n_next = d_steps + 2 * L;
+    tp.u_cnt = d_cnts;
+    tp.p_cnt = d_cnts + L;
+#define MPX_CUDA_REL(call)                                                                                          \
+    do {                                                                                                            \
+        cudaError_t e2_ = (call);                                                                                   \
+        if (e2_ != cudaSuccess) {                                                                                   \
+            release();                                                                                              \
+            return fail(eng, MPX_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e2_));                     \
+        }                                                                                                           \
+    } while (0)
+    MPX_CUDA_REL(cudaMemcpyAsync(d_steps, u_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA_REL(cudaMemcpyAsync(d_steps + L, p_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA_REL(cudaMemcpyAsync(d_steps + 2 * L, n_next.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA_REL(cudaMemsetAsync(d_cnts, 0, 2 * L * sizeof(unsigned long long), e->stream));
+    MPX_CUDA_REL(cudaMemsetAsync(grad, 0, L * sizeof(double), e->stream));
+    MPX_CUDA_REL(cudaMemsetAsync(done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+    pick_adj_init(e->W, e->cfg.basis)(e, lam, nf);
+    const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
+    for (size_t sg = S; sg-- > 0;) {
+        const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
+        const uint64_t n = A.ck_n[sg];
+        if (n > 0)
+            MPX_CUDA_REL(cudaMemcpyAsync(e->st.coef, A.ck_coef[sg], n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         e->stream));
+        Counters c{};
+        c.n = n;
+        c.n0 = n;
+        c.stall = kNoStall;
+        MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+        for (uint64_t st = lo; st < hi; ++st) replay(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), tp);
+        for (uint64_t st = hi; st-- > lo;) {
+            const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
+            k_adj_pairs<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
+            k_adj_undo<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
+        }
+        e->launches += 5 * (hi - lo);
+        MPX_CUDA_REL(cudaGetLastError());
+    }
+    e->launches += 1;
+    // the engine keeps the evolved operator of the forward pass
+    if (nf > 0)
+        MPX_CUDA_REL(cudaMemcpyAsync(e->st.coef, A.final_coef, nf * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    MPX_CUDA_REL(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA_REL(cudaMemcpyAsync(grad_angles, grad, L * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA_REL(cudaStreamSynchronize(e->stream));
+    const uint32_t err = e->h_cnt->err;
+    Counters c{};
+    c.n = nf;
+    c.n0 = nf;
+    c.stall = kNoStall;
+    MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+    release();
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+#undef MPX_CUDA_REL
+    if (err != 0) return fail(eng, MPX_ERR_STATE, "gradient replay diverged from the forward pass (internal error)");
     return MPX_OK;
 }
 
@@ -486,7 +747,7 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     e->device = cfg->device;
     e->core = core;
     for (int w = 0; w < e->W; ++w) e->mask.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
-    e->grid = std::min(prop.multiProcessorCount * 8, kMaxGrid);
+    e->grid = prop.multiProcessorCount * 8;
     mpx_engine *eng = e;
     auto bail = [&](mpx_status st) {
         g_create_error = e->err;
@@ -502,8 +763,6 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.q_count), e->grid * sizeof(uint32_t));
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_anti), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_out), sizeof(double));
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_out), sizeof(double));
@@ -666,6 +925,7 @@ mpx_status mpx_reset(mpx_engine *e) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     mpx_engine *eng = e;
     MPX_CUDA(cudaSetDevice(e->device));
+    free_adjoint(e);
     return load_initial(e);
 }
 
@@ -718,17 +978,41 @@ mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out) {
     return MPX_OK;
 }
 
+mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation) {
+    if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    MPX_CUDA(cudaSetDevice(e->device));
+    mpx_status s = adjoint_forward(e, *c, segment_gates);
+    if (s != MPX_OK) return s;
+    return mpx_expectation(e, expectation);
+}
+
+mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *grad_angles) {
+    if (e == nullptr || c == nullptr || (c->n > 0 && grad_angles == nullptr))
+        return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    if (e->adj.circuit != c || e->adj.L != c->n)
+        return fail(eng, MPX_ERR_STATE, "mpx_adjoint_backward needs a preceding mpx_adjoint_forward of the same circuit "
+                                        "with no propagation in between");
+    MPX_CUDA(cudaSetDevice(e->device));
+    if (c->n == 0) return MPX_OK;
+    return adjoint_backward(e, *c, grad_angles);
+}
+
 mpx_status mpx_set_profiling(mpx_engine *e, int32_t on) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     e->profile = on != 0;
     return MPX_OK;
 }
 
-mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, uint64_t *n_gates) {
+mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, double *columns_ms,
+                            uint64_t *n_gates) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     if (!e->profile) return fail(e, MPX_ERR_STATE, "profiling is off (mpx_set_profiling)");
     if (sweep_ms) *sweep_ms = e->t_sweep_ms;
     if (resolve_ms) *resolve_ms = e->t_resolve_ms;
+    if (columns_ms) *columns_ms = e->t_columns_ms;
     if (n_gates) *n_gates = e->n_sweep;
     return MPX_OK;
 }
@@ -741,6 +1025,8 @@ void mpx_destroy(mpx_engine *e) {
         cudaSetDevice(e->device);
         cudaStreamSynchronize(e->stream);
     }
+    free_adjoint(e);
+    cudaStreamSynchronize(e->stream);
     free_store(e);
     cudaFree(e->d_cnt);
     cudaFreeHost(e->h_cnt);
@@ -748,8 +1034,6 @@ void mpx_destroy(mpx_engine *e) {
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
     for (auto &ev : e->pev) cudaEventDestroy(ev);
-    cudaFree(e->sc.q_count);
-    cudaFree(e->sc.blk_anti);
     cudaFree(e->d_partial);
     cudaFree(e->d_out);
     cudaFreeHost(e->h_out);

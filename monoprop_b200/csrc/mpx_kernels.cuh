@@ -1,34 +1,58 @@
 // mpx_kernels.cuh -- the per-gate kernels of the B200 propagation engine (sm_100a).
 //
-// One Heisenberg gate = two launches over the device term store:
-//   k_sweep   -- streams every key once (HBM-bound): anticommutation parity, fused cos scaling of the
-//                anticommuting coefficients, lower_atol / structural-cutoff / upper_atol emit gate,
-//                rotation phase, leader/follower class; compacts the emitted sine branches into per-block
-//                query regions (no global atomics) and writes the leader-emitted bitmap.
+// One Heisenberg gate = three launches over the device term store:
+//   k_sweep   -- anticommutation test from the generator's bit-columns (|fold| bits per term), fused cos
+//                scaling of the anticommuting coefficients, lower_atol / structural-cutoff / upper_atol
+//                emit gate, rotation phase, leader/follower class; compacts the emitted sine branches into
+//                the query arrays and writes the leader-emitted bitmap.
 //   k_resolve -- one thread per emitted branch: open-addressing lookup of the partner M^G, the
 //                leader/follower rule, the rotation of the pair, or the unique append of the missing partner.
+//   k_columns -- adds the appended terms to the bit-columns.
 // Every coefficient slot is written by exactly one thread per gate (the sine partner map M -> M^G is
 // injective), so no coefficient atomics are needed (layer_build/FusedApply.h:54-56).
 #pragma once
 
 #include <cstdint>
 
+#include "mpx_adjoint.cuh"
 #include "mpx_device.cuh"
 
 namespace mpx {
 
-__device__ __forceinline__ uint64_t region_size(uint64_t n0, uint32_t grid) {
-    const uint64_t per = (n0 + grid - 1) / grid;
-    return (per + kBlock - 1) / kBlock * kBlock;
+// Index (0-based) of the r-th set bit of a (r < popc(a)), by popcount bisection.
+__device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
+    int pos = 0;
+#pragma unroll
+    for (int width = 16; width >= 1; width >>= 1) {
+        const int c = __popc(a & ((1u << width) - 1u));
+        if (r >= c) {
+            r -= c;
+            a >>= width;
+            pos += width;
+        }
+    }
+    return pos;
 }
 
-// Fused scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
-template <int W, int BASIS>
+constexpr int kWarps = kBlock / 32;
+
+// Fused anticommutation scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
+// Each warp owns chunks of 1024 terms (32 column words). The anticommutation bit of 32 terms at once is
+// the XOR of the generator's fold columns (Pauli pair_swap(G), Majorana G, plus the |M|-parity column
+// for odd |G|): only |fold| bits per term are read, not the 8W-byte key. The anticommuting terms of the
+// chunk are then spread over the 32 lanes (prefix sums + popcount bisection); each is cos-scaled, and
+// only those that pass the lower_atol gate load their key row to build the partner M^G, run the
+// structural cutoff / upper_atol rescue and the rotation phase. Emitted branches are appended to the
+// query arrays through one atomic per warp round. In REPLAY mode (a segment re-run for the gradient)
+// every anticommuting term's index and pre-gate coefficient also go to the tape's undo log.
+template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
-                                                   Trunc tr) {
-    __shared__ uint32_t warp_tot[kBlock / 32];
-    __shared__ uint32_t warp_anti[kBlock / 32];
+                                                   Trunc tr, Tape tp) {
+    __shared__ uint32_t s_anti[kWarps][32];
+    __shared__ uint32_t s_foll[kWarps][32];
+    __shared__ uint32_t s_pfx[kWarps][32];
+    __shared__ uint32_t s_emit[kWarps][32];
     if (cnt->stall != kNoStall) return;
     const uint64_t n0 = cnt->n;
     if (2 * n0 > st.cap) {
@@ -37,61 +61,87 @@ __global__ void __launch_bounds__(kBlock) k_sweep(Store st, Scratch sc, Counters
         if (threadIdx.x == 0) atomicMin(&cnt->stall, step);
         return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n0 = n0;
+    const uint32_t par = step & 1u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt->n0 = n0;
+        cnt->q_total[par ^ 1u] = 0;
+        cnt->anti[par ^ 1u] = 0;
+    }
     const GateDesc &gd = gates[gate];
+    if (gd.empty || n0 == 0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    if (gd.empty) {
-        if (threadIdx.x == 0) {
-            sc.q_count[blockIdx.x] = 0;
-            sc.blk_anti[blockIdx.x] = 0;
-        }
-        return;
-    }
-    uint64_t g[W], fold[W], pmask[W];
+    uint64_t g[W];
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-        g[w] = gd.g[w];
-        fold[w] = gd.fold[w];
-        pmask[w] = (w == gd.pivot_word) ? gd.pivot_bit : 0ULL;
-    }
+    for (int w = 0; w < W; ++w) g[w] = gd.g[w];
     const double cosv = gd.cosv, sinabs = gd.abs_sin;
     const bool cos_zero = gd.cos_zero != 0;
     const int gpop = gd.gpop;
+    const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(gd.pivot_col) * st.cstride;
+    const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
+    const uint64_t nwords = (n0 + 31) >> 5;
+    const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
+    uint32_t anti_count = 0;
 
-    const uint64_t T = region_size(n0, gridDim.x);
-    const uint64_t begin = static_cast<uint64_t>(blockIdx.x) * T;
-    const uint64_t end = min(begin + T, n0);
-    uint32_t count = 0, anti_total = 0;
-    for (uint64_t base = begin; base < end; base += kBlock) {
-        const uint64_t i = base + threadIdx.x;
-        bool anti = false, emit = false, foll = false;
-        int phase = 0;
-        double v = 0.0;
-        if (i < end) {
-            uint64_t m[W];
-            load_key<W>(st.keys, i, m);
-            uint64_t par = 0, pv = 0;
-            int mpop = 0;
+    for (uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * kWarps + warp; chunk * 32 < nwords;
+         chunk += static_cast<uint64_t>(gridDim.x) * kWarps) {
+        const uint64_t j = chunk * 32 + lane;
+        uint32_t anti = 0, foll = 0;
+        if (j < nwords) {
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                par ^= m[w] & fold[w];
-                pv |= m[w] & pmask[w];
-                mpop += __popcll(m[w]);
+                for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
+                    const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
+                    anti ^= st.cols[c * st.cstride + j];
+                }
             }
-            anti = ((__popcll(par) ^ (gd.g_odd & mpop)) & 1) != 0;
-            if (anti) {
-                foll = pv != 0;
-                v = st.coef[i];
-                st.coef[i] = v * cosv;
-                if (cos_zero) sc.aux[i] = v;
+            if (gd.g_odd) anti ^= parity[j];
+            if (j == nwords - 1) anti &= tail;
+            foll = anti & pivot[j];
+        }
+        const int cnt_l = __popc(anti);
+        int incl = cnt_l;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        anti_count += static_cast<uint32_t>(cnt_l);
+        s_anti[warp][lane] = anti;
+        s_foll[warp][lane] = foll;
+        s_pfx[warp][lane] = static_cast<uint32_t>(incl - cnt_l);
+        s_emit[warp][lane] = 0;
+        __syncwarp();
+        for (int k = 0; k < total; k += 32) {
+            const int idx = k + lane;
+            bool emit = false, follower = false;
+            int phase = 0, owner = 0, bit = 0;
+            double v = 0.0;
+            uint64_t term = 0;
+            if (idx < total) {
+                int lo = 0, hi = 32;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
+                    else hi = mid;
+                }
+                owner = lo;
+                bit = nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
+                follower = (s_foll[warp][lo] >> bit) & 1u;
+                term = (chunk * 32 + static_cast<uint64_t>(lo)) * 32 + static_cast<uint64_t>(bit);
+                v = st.coef[term];
+                st.coef[term] = v * cosv;
+                if (cos_zero) sc.aux[term] = v;
                 const double av = fabs(v);
                 if (!(tr.has_lower && sinabs * av <= tr.lower)) {
-                    uint64_t p[W];
-                    int ov = 0;
+                    uint64_t m[W], p[W];
+                    load_key<W>(st.keys, term, m);
+                    int mpop = 0, ov = 0;
 #pragma unroll
                     for (int w = 0; w < W; ++w) {
                         p[w] = m[w] ^ g[w];
+                        mpop += __popcll(m[w]);
                         ov += __popcll(m[w] & g[w]);
                     }
                     const int ppop = mpop + gpop - 2 * ov;
@@ -101,102 +151,61 @@ __global__ void __launch_bounds__(kBlock) k_sweep(Store st, Scratch sc, Counters
                     }
                 }
             }
+            if constexpr (REPLAY) {
+                const uint32_t vb = __ballot_sync(0xFFFFFFFFu, idx < total);
+                unsigned long long ub = 0;
+                if (lane == 0) ub = atomicAdd(&tp.u_cnt[step], static_cast<unsigned long long>(__popc(vb)));
+                ub = __shfl_sync(0xFFFFFFFFu, ub, 0);
+                if (idx < total) {
+                    const uint64_t r = tp.u_base[step] + ub + __popc(vb & lt_mask);
+                    tp.u_idx[r] = static_cast<uint32_t>(term);
+                    tp.u_val[r] = v;
+                }
+            }
+            const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
+            if (eb != 0) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(&cnt->q_total[par], static_cast<unsigned long long>(__popc(eb)));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (emit) {
+                    const uint64_t q = base + __popc(eb & lt_mask);
+                    sc.q_src[q] = static_cast<uint32_t>(term);
+                    sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
+                    sc.q_val[q] = v;
+                    if (!follower) atomicOr(&s_emit[warp][owner], 1u << bit);
+                }
+            }
         }
-        const uint32_t lead_ball = __ballot_sync(0xFFFFFFFFu, emit && !foll);
-        const uint32_t emit_ball = __ballot_sync(0xFFFFFFFFu, emit);
-        const uint32_t anti_ball = __ballot_sync(0xFFFFFFFFu, anti);
-        const uint64_t wbase = base + static_cast<uint64_t>(warp) * 32;
-        if (lane == 0) {
-            if (wbase < end) sc.emit_bits[wbase >> 5] = lead_ball;
-            warp_tot[warp] = __popc(emit_ball);
-            warp_anti[warp] = __popc(anti_ball);
-        }
-        __syncthreads();
-        uint32_t off = 0, tot = 0, atot = 0;
+        __syncwarp();
+        if (j < nwords) sc.emit_bits[j] = s_emit[warp][lane];
+        __syncwarp();
+    }
 #pragma unroll
-        for (int w = 0; w < kBlock / 32; ++w) {
-            const uint32_t t = warp_tot[w];
-            off += (w < warp) ? t : 0u;
-            tot += t;
-            atot += warp_anti[w];
-        }
-        if (emit) {
-            const uint64_t q = begin + count + off + __popc(emit_ball & lt_mask);
-            sc.q_src[q] = static_cast<uint32_t>(i);
-            sc.q_flag[q] = static_cast<uint8_t>((foll ? 1 : 0) | (phase_code(phase) << 1));
-            sc.q_val[q] = v;
-        }
-        count += tot;
-        anti_total += atot;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        sc.q_count[blockIdx.x] = count;
-        sc.blk_anti[blockIdx.x] = anti_total;
-    }
+    for (int o = 16; o > 0; o >>= 1) anti_count += __shfl_down_sync(0xFFFFFFFFu, anti_count, o);
+    if (lane == 0 && anti_count != 0) atomicAdd(&cnt->anti[par], static_cast<unsigned long long>(anti_count));
 }
-
-// Exclusive scan of the per-block query counts into s_off[0..grid] (s_off[grid] = total).
-__device__ __forceinline__ void scan_counts(const uint32_t *__restrict__ counts, uint32_t grid, uint64_t *s_off,
-                                            uint64_t *s_part) {
-    const uint32_t per = (grid + kBlock - 1) / kBlock;
-    const uint32_t lo = threadIdx.x * per;
-    uint64_t sum = 0;
-    for (uint32_t k = 0; k < per; ++k) {
-        const uint32_t j = lo + k;
-        if (j < grid) sum += counts[j];
-    }
-    s_part[threadIdx.x] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint64_t acc = 0;
-        for (int t = 0; t < kBlock; ++t) {
-            const uint64_t x = s_part[t];
-            s_part[t] = acc;
-            acc += x;
-        }
-        s_off[grid] = acc;
-    }
-    __syncthreads();
-    uint64_t acc = s_part[threadIdx.x];
-    for (uint32_t k = 0; k < per; ++k) {
-        const uint32_t j = lo + k;
-        if (j < grid) {
-            s_off[j] = acc;
-            acc += counts[j];
-        }
-    }
-    __syncthreads();
-}
-
-constexpr int kMaxGrid = 148 * 8;
 
 // Partner resolve + rotation apply + append (Engine.h:364-513, FusedApply.h:32-83, MPOperator.h:269-278).
-template <int W, int BASIS>
+// In REPLAY mode the keys of this gate's appends already exist (indices >= n0, inserted by the forward
+// pass): a partner found there is treated as the append it was, nothing is inserted, and every rotated
+// or appended pair goes to the tape's pair log with both pre-gate coefficients.
+template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
-                                                     uint64_t *__restrict__ stats) {
-    __shared__ uint64_t s_off[kMaxGrid + 1];
-    __shared__ uint64_t s_part[kBlock];
-    __shared__ uint32_t warp_miss[kBlock / 32];
+                                                     uint64_t *__restrict__ stats, Tape tp) {
+    __shared__ uint32_t warp_miss[kWarps];
     __shared__ unsigned long long s_base;
     if (cnt->stall != kNoStall) return;
+    const uint32_t par = step & 1u;
     const uint64_t n0 = cnt->n0;
+    const uint64_t total = cnt->q_total[par];
     const GateDesc &gd = gates[gate];
-    const uint32_t grid = gridDim.x;
-    scan_counts(sc.q_count, grid, s_off, s_part);
-    const uint64_t total = s_off[grid];
-    if (blockIdx.x == 0) {
-        if (threadIdx.x == 0) {
-            uint64_t a = 0;
-            for (uint32_t b = 0; b < grid; ++b) a += sc.blk_anti[b];
-            stats[4 * static_cast<uint64_t>(step) + 0] = n0;
-            stats[4 * static_cast<uint64_t>(step) + 1] = gd.empty ? 0 : a;
-            stats[4 * static_cast<uint64_t>(step) + 2] = total;
-        }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        stats[4 * static_cast<uint64_t>(step) + 0] = n0;
+        stats[4 * static_cast<uint64_t>(step) + 1] = cnt->anti[par];
+        stats[4 * static_cast<uint64_t>(step) + 2] = total;
     }
     if (total == 0) return;
-    const uint64_t T = region_size(n0, grid);
     uint64_t g[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) g[w] = gd.g[w];
@@ -206,22 +215,14 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
     const uint32_t lt_mask = (1u << lane) - 1u;
 
     for (uint64_t tb = static_cast<uint64_t>(blockIdx.x) * kBlock; tb < total;
-         tb += static_cast<uint64_t>(grid) * kBlock) {
-        const uint64_t k = tb + threadIdx.x;
+         tb += static_cast<uint64_t>(gridDim.x) * kBlock) {
+        const uint64_t q = tb + threadIdx.x;
         bool miss = false;
         uint64_t p[W];
         uint64_t pos = 0;
         uint32_t tag = 0;
         double v = 0.0, ph = 0.0;
-        if (k < total) {
-            // region r holding global query k: the last r with s_off[r] <= k
-            uint32_t lo = 0, hi = grid;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (s_off[mid] <= k) lo = mid;
-                else hi = mid;
-            }
-            const uint64_t q = static_cast<uint64_t>(lo) * T + (k - s_off[lo]);
+        if (q < total) {
             const uint32_t src = sc.q_src[q];
             const uint8_t flag = sc.q_flag[q];
             v = sc.q_val[q];
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     break;
                 }
                 const uint32_t idx = static_cast<uint32_t>(slot);
-                if (idx < n0 && static_cast<uint32_t>(slot >> 32) == tag) {
+                if ((REPLAY || idx < n0) && static_cast<uint32_t>(slot >> 32) == tag) {
                     uint64_t o[W];
                     load_key<W>(st.keys, idx, o);
                     bool eq = true;
@@ -260,6 +261,22 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 }
                 pos = (pos + 1) & st.tmask;
             }
+            if constexpr (REPLAY) {
+                if (miss) { // the forward pass found or appended every partner of this gate
+                    atomicOr(&cnt->err, 8u);
+                    miss = false;
+                }
+                else if (!gave_up && found >= n0) {
+                    st.coef[found] = (sinv * ph) * v;
+                    const uint64_t r = tp.p_base[step] + atomicAdd(&tp.p_cnt[step], 1ULL);
+                    tp.p_src[r] = src;
+                    tp.p_tgt[r] = static_cast<uint32_t>(found);
+                    tp.p_code[r] = static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF));
+                    tp.p_vs[r] = v;
+                    tp.p_vt[r] = 0.0;
+                    gave_up = true; // handled
+                }
+            }
             if (!miss && !gave_up) {
                 const bool follower = (flag & 1) != 0;
                 const bool leader_took_it = follower && ((sc.emit_bits[found >> 5] >> (found & 31)) & 1u);
@@ -267,6 +284,14 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     const double vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
                     st.coef[src] = __fma_rn(sinv * -ph, vt, st.coef[src]);
                     st.coef[found] = __fma_rn(sinv * ph, v, st.coef[found]);
+                    if constexpr (REPLAY) {
+                        const uint64_t r = tp.p_base[step] + atomicAdd(&tp.p_cnt[step], 1ULL);
+                        tp.p_src[r] = src;
+                        tp.p_tgt[r] = static_cast<uint32_t>(found);
+                        tp.p_code[r] = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
+                        tp.p_vs[r] = v;
+                        tp.p_vt[r] = vt;
+                    }
                 }
             }
         }
@@ -276,7 +301,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
         __syncthreads();
         uint32_t off = 0, tot = 0;
 #pragma unroll
-        for (int w = 0; w < kBlock / 32; ++w) {
+        for (int w = 0; w < kWarps; ++w) {
             const uint32_t t = warp_miss[w];
             off += (w < warp) ? t : 0u;
             tot += t;
@@ -299,6 +324,53 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
             }
         }
         __syncthreads();
+    }
+}
+
+// Writes the bit-columns of terms [lo, hi): one warp per 32-term column word, one ballot per key bit.
+// A word that starts below lo already holds valid bits for the terms below lo (and zeros above) and is
+// OR-ed; every other word is assigned whole, so no clearing is ever needed. With from_counters the range
+// is the current gate's appends [n0, n).
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_columns(Store st, const Counters *__restrict__ cnt, uint64_t lo,
+                                                     uint64_t hi, int from_counters) {
+    if (from_counters) {
+        if (cnt->stall != kNoStall) return;
+        lo = cnt->n0;
+        hi = cnt->n;
+    }
+    if (hi <= lo) return;
+    const int lane = threadIdx.x & 31;
+    const uint64_t w1 = (hi + 31) >> 5;
+    for (uint64_t j = (lo >> 5) + (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; j < w1;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x / 32) {
+        const uint64_t i = j * 32 + lane;
+        uint64_t m[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) m[w] = 0;
+        if (i >= lo && i < hi) load_key<W>(st.keys, i, m);
+        const bool boundary = j * 32 < lo;
+        uint32_t mine[2 * W];
+        int pop = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            pop += __popcll(m[w]);
+#pragma unroll
+            for (int b = 0; b < 64; ++b) {
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (m[w] >> b) & 1ULL);
+                if (lane == (b & 31)) mine[2 * w + (b >> 5)] = bal;
+            }
+        }
+        const uint32_t par = __ballot_sync(0xFFFFFFFFu, pop & 1);
+#pragma unroll
+        for (int r = 0; r < 2 * W; ++r) {
+            uint32_t *dst = st.cols + static_cast<uint64_t>(32 * r + lane) * st.cstride + j;
+            *dst = boundary ? (*dst | mine[r]) : mine[r];
+        }
+        if (lane == 0) {
+            uint32_t *dst = st.cols + static_cast<uint64_t>(64 * W) * st.cstride + j;
+            *dst = boundary ? (*dst | par) : par;
+        }
     }
 }
 

@@ -132,17 +132,23 @@ def kicked_ising(nx: int, ny: int, layers: int, seed: int, theta_max: float,
     return slots, g, pmap, params
 
 
+def _per_layer(edges_n: int, sites: int) -> dict:
+    return {"gates_per_layer": edges_n + sites}
+
+
 def line20(seed: int = 1234, layers: int = 10) -> Workload:
     n = 20
     edges = [(i, i + 1) for i in range(n - 1)]
     slots, g, pmap, params = kicked_ising(n, 1, layers, seed, np.pi, edges)
-    return Workload("line20", "pauli", n, slots, g, pmap, params, {(20, 21): 1.0 + 0j}, [], 8, "support", 1e-4)
+    return Workload("line20", "pauli", n, slots, g, pmap, params, {(20, 21): 1.0 + 0j}, [], 8, "support", 1e-4,
+                    extra=_per_layer(n - 1, n))
 
 
 def ising100(seed: int = 1234, layers: int = 20) -> Workload:
     slots, g, pmap, params = kicked_ising(10, 10, layers, seed, 0.3 * np.pi)
     obs = {(2 * i, 2 * i + 1): 0.01 + 0j for i in range(100)}
-    return Workload("ising100", "pauli", 100, slots, g, pmap, params, obs, [], 10, "support", 1e-5)
+    return Workload("ising100", "pauli", 100, slots, g, pmap, params, obs, [], 10, "support", 1e-5,
+                    extra=_per_layer(180, 100))
 
 
 def ising50(depth: int, seed: int = 99, observable_qubit: int | None = None) -> Workload:
@@ -150,7 +156,7 @@ def ising50(depth: int, seed: int = 99, observable_qubit: int | None = None) -> 
     q = observable_qubit if observable_qubit is not None else int(np.random.default_rng(seed + 1).integers(0, 50))
     obs = {(2 * q, 2 * q + 1): 1.0 + 0j}
     return Workload(f"ising50_d{depth}", "pauli", 50, slots, g, pmap, params, obs, [], 8, "support", 1e-5,
-                    extra={"observable_qubit": q, "depth": depth})
+                    extra={"observable_qubit": q, "depth": depth, **_per_layer(85, 50)})
 
 
 def hubbard6x6(seed: int = 7, steps: int = 8, lx: int = 6, ly: int = 6) -> Workload:
@@ -180,7 +186,8 @@ def hubbard6x6(seed: int = 7, steps: int = 8, lx: int = 6, ly: int = 6) -> Workl
     obs = {(): 0.5 + 0j, (0, 1): 0.5j}
     state = [2 * s + (s % 2) for s in range(sites)]
     return Workload("hubbard6x6", "majorana", 2 * sites, slots, np.asarray(g), np.asarray(pmap, dtype=np.int64),
-                    np.asarray(params), obs, state, 8, "length", 1e-5)
+                    np.asarray(params), obs, state, 8, "length", 1e-5,
+                    extra={"gates_per_layer": 2 * 2 * len(bonds) + sites})
 
 
 def batch_ising50(n_instances: int = 256, seed: int = 99, min_depth: int = 4, max_depth: int = 24) -> list[Workload]:

@@ -7,6 +7,10 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
   coefficients exported at the C++ level (not the rounded ``evolved_operator`` dict), keys sorted
   canonically, ``<0|O|0>``; bigger stores keep only a digest: term count, SHA-256 of the sorted keys,
   sum and sum of squares of the coefficients in key order;
+* ``grad_<workload>.npz`` -- the reference's gradient of the frozen-structure surrogate (graph built with
+  the same parameters, then ``expectation_value_and_gradient``), per parameter;
+* ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
+  replayed graph;
 * ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
   (``tests/data/{rx_rz_ry_rz_exact,random_exact,lih_fermionic_spin_exact}.msgpack``), re-expressed as
   engine arrays by this repository's front-end (``Circuit.from_dense_arrays`` + ``expand_monomials``,
@@ -47,6 +51,18 @@ SEEDED = [
 ]
 
 REF_CASES = ["rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact"]
+
+# Gradients of the frozen-structure surrogate from the reference's graph replay (build_graph seeded
+# with the same parameters, then expectation_value_and_gradient): grad_<name>.npz. These circuits keep
+# |cos(2 angle)| >= 0.58; the 20-qubit line circuit (angles up to pi) has a gate with |cos| = 1.2e-4,
+# where the reference's analytic gradient (which un-scales by 1/cos) loses accuracy, so its golden
+# gradient is the parameter shift of the replayed graph instead (pshift_line20.npz).
+GRADS = [
+    ("hubbard6x6_L300", W.hubbard6x6, 300),
+    ("ising100_L600", W.ising100, 600),
+    ("ising50_d2", lambda: W.ising50(2), None),
+    ("ising100", W.ising100, None),  # the full 100-qubit, 5600-angle circuit (about a minute here)
+]
 
 
 def digest(keys: np.ndarray, coefs: np.ndarray) -> dict:
@@ -89,6 +105,37 @@ def main(reference_root: str = "/root/reference") -> None:
         save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
                     {"n_layers": np.int64(wl.n_layers if L is None else L)})
         print(name, r.keys.shape[0], r.expectation)
+    for name, make, L in GRADS:
+        wl = make()
+        n_layers = wl.n_layers if L is None else L
+        eng = oracle.RefEngine(wl, partitions=8 if name == "ising100" else 1)
+        eng.propagate(n_layers=L, build_graph=True)
+        n_params = int(wl.param_map[:n_layers].max()) + 1
+        ev, grad, _ = eng.expectation_and_gradient(wl.params[:n_params])
+        eng.close()
+        np.savez_compressed(os.path.join(HERE, f"grad_{name}.npz"), expectation=np.float64(ev), grad=grad,
+                            n_layers=np.int64(n_layers), n_params=np.int64(n_params))
+        print("grad", name, ev, float(np.abs(grad).max()))
+    # Parameter-shift gradient of the 20-qubit line circuit from the reference's replayed graph: each
+    # replayed layer is affine in (cos 2 g theta, sin 2 g theta), so E(theta + s e_p) - E(theta - s e_p)
+    # with s = pi / (4 |g|) times |g| is the exact derivative of the frozen surrogate (one layer per
+    # parameter here).
+    wl = W.line20()
+    eng = oracle.RefEngine(wl)
+    eng.propagate(build_graph=True)
+    theta = wl.params.copy()
+    ps = np.zeros_like(theta)
+    for p in range(theta.size):
+        g = abs(float(wl.gen_coeffs[p]))
+        s = np.pi / (4 * g)
+        tp, tm = theta.copy(), theta.copy()
+        tp[p] += s
+        tm[p] -= s
+        ps[p] = g * (eng.expectation(tp) - eng.expectation(tm))
+    ev0 = eng.expectation(theta)
+    eng.close()
+    np.savez_compressed(os.path.join(HERE, "pshift_line20.npz"), expectation=np.float64(ev0), grad=ps)
+    print("pshift line20", ev0, float(np.abs(ps).max()))
     for case in REF_CASES:
         for tag, la in (("", None), ("_atol1e-10", 1e-10)):
             wl, exact, grad = fixture_workload(case, reference_root, la)
