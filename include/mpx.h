@@ -146,6 +146,12 @@ MPX_API mpx_status mpx_set_profiling(mpx_engine *e, int32_t on);
 MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, double *columns_ms,
                                     uint64_t *n_gates);
 
+/* Device memory of all engines on a device comes from one library-owned pool that keeps freed memory
+ * mapped for reuse (so creating engines and regrowing stores does not re-map gigabytes each time). This
+ * returns the cached, unused part of that pool to the driver. No reference counterpart (the reference
+ * is host-only). */
+MPX_API mpx_status mpx_trim_device_memory(int32_t device);
+
 MPX_API const char *mpx_last_error(const mpx_engine *e);
 
 /* <0|O|0> of a term store the caller holds in device memory, computed without allocating any device

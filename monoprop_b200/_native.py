@@ -23,7 +23,7 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_set_profiling", "mpx_kernel_times",
-            "mpx_last_error",
+            "mpx_trim_device_memory", "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc")
 
 
@@ -82,6 +82,7 @@ def load() -> C.CDLL:
             "mpx_set_profiling": (st, [vp, C.c_int32]),
             "mpx_kernel_times": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(u64)]),
+            "mpx_trim_device_memory": (st, [C.c_int32]),
             "mpx_last_error": (C.c_char_p, [vp]),
             "mpx_destroy": (None, [vp]),
             "mpx_expectation_noalloc": (st, [C.c_int32, C.c_uint32, vp, vp, u64, vp, C.c_double, vp, vp, C.c_char_p,

@@ -23,8 +23,10 @@
 
 namespace mpx {
 
-// Logs written by a replayed segment, indexed by the step's offsets (per-step bases are prefix sums of
-// the forward pass's a_g and e_g, so a step's records are contiguous).
+// Logs written by a replayed segment. A step's records are contiguous (per-step bases are prefix sums
+// of the forward pass's a_g and e_g). Undo records are placed without atomics: the forward pass saves
+// every sweep warp's anticommuting count per step (w_anti), a prefix scan turns them into per-warp
+// offsets (u_off), and the replayed warp writes its records in its own scan order from there.
 struct Tape {
     uint32_t *u_idx; // undo log: anticommuting term index
     double *u_val;   //           its coefficient before the gate
@@ -33,12 +35,43 @@ struct Tape {
     int8_t *p_code;  //           phase (+1 / -1 / 0) | 0x10 when T was appended by this gate
     double *p_vs;    //           c_S before the gate
     double *p_vt;    //           c_T before the gate (0 for an append)
-    const uint64_t *u_base; // [n_steps] first undo record of each step
-    const uint64_t *p_base; // [n_steps] first pair record of each step
-    unsigned long long *u_cnt; // [n_steps] undo records written per step
+    const uint64_t *u_base;    // [n_steps] first undo record of each step
+    const uint64_t *p_base;    // [n_steps] first pair record of each step
+    unsigned long long *u_cnt; // [n_steps] undo records per step (filled by the offset scan)
     unsigned long long *p_cnt; // [n_steps] pair records written per step
     const uint64_t *n_next;    // [n_steps] store size after each step (from the forward pass)
+    uint32_t *w_anti;          // forward pass: [n_steps][sweep warps] anticommuting terms per warp
+    const uint64_t *u_off;     // replay: [steps of the segment][sweep warps] first undo record per warp
+    uint64_t u_off_step0;      // step of u_off's first row
 };
+
+// Per step of a segment: exclusive prefix over the sweep warps' anticommuting counts -> undo offsets
+// (one block per step, fixed order).
+__global__ void __launch_bounds__(1024) k_undo_offsets(Tape tp, uint32_t n_warps, uint64_t step_lo,
+                                                        uint64_t *__restrict__ u_off) {
+    __shared__ uint64_t s_part[1024];
+    const uint64_t step = step_lo + blockIdx.x;
+    const uint32_t *src = tp.w_anti + step * n_warps;
+    const uint32_t per = (n_warps + blockDim.x - 1) / blockDim.x;
+    const uint32_t lo = threadIdx.x * per;
+    uint64_t sum = 0;
+    for (uint32_t k = 0; k < per && lo + k < n_warps; ++k) sum += src[lo + k];
+    s_part[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t o = 1; o < blockDim.x; o <<= 1) {
+        const uint64_t t = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
+        __syncthreads();
+        s_part[threadIdx.x] += t;
+        __syncthreads();
+    }
+    uint64_t acc = tp.u_base[step] + (threadIdx.x > 0 ? s_part[threadIdx.x - 1] : 0);
+    uint64_t *dst = u_off + static_cast<uint64_t>(blockIdx.x) * n_warps;
+    for (uint32_t k = 0; k < per && lo + k < n_warps; ++k) {
+        dst[lo + k] = acc;
+        acc += src[lo + k];
+    }
+    if (threadIdx.x == blockDim.x - 1) tp.u_cnt[step] = s_part[threadIdx.x];
+}
 
 __device__ __forceinline__ double block_sum(double v, double *s_red) {
 #pragma unroll

@@ -15,6 +15,7 @@ constexpr uint64_t kEven = 0x5555555555555555ULL;
 constexpr unsigned long long kEmptySlot = ~0ULL;
 constexpr uint32_t kNoStall = 0xFFFFFFFFu;
 constexpr int kBlock = 256;
+constexpr int kMaxFoldCols = 8; // fold columns read with independent loads; wider generators loop
 
 // Per-gate constants, precomputed on the host once per circuit (cos/sin through the host libm, the
 // same calls the reference makes: layer_build/Engine.h:555-560, FusedApply.h:45-46).
@@ -27,7 +28,8 @@ struct GateDesc {
     uint64_t pivot_bit;
     int32_t cos_zero, empty;
     int32_t pivot_col; // physical bit index of the pivot: 64 * pivot_word + ctz(pivot_bit)
-    int32_t pad;
+    int32_t n_fold;    // number of fold columns (set bits of fold)
+    uint16_t fold_cols[kMaxFoldCols]; // their physical bit indices, when n_fold <= kMaxFoldCols
 };
 
 // Engine-wide truncation settings (CutoffContext.h:20-42, AlgebraCommon.h:229-243).
@@ -44,10 +46,6 @@ struct Counters {
     unsigned long long n0; // term count at the start of the current gate
     uint32_t stall;        // kNoStall, or the step index at which capacity ran out
     uint32_t err;          // nonzero: a bounded probe loop gave up (table inconsistent); results invalid
-    // Per-gate query and anticommuting-term counts, double-buffered by step parity: the sweep of step s
-    // accumulates into [s & 1] and clears [(s + 1) & 1] for the next gate.
-    unsigned long long q_total[2];
-    unsigned long long anti[2];
 };
 
 struct StateMask {
@@ -68,10 +66,17 @@ struct Store {
     uint64_t cap;     // term capacity
 };
 
+// Emitted sine branches of the current gate. Warp w of the sweep grid owns the query region
+// [w * stride, w * stride + q_count[w]), stride = (chunks per warp) * 1024 >= the terms it scans, so no
+// two warps ever contend for a slot or a counter; the resolve block b takes the regions of the sweep
+// block b's warps.
 struct Scratch {
-    uint32_t *q_src;     // emitted sine branches of the current gate, in any order
+    uint32_t *q_src;     // source term index
     uint8_t *q_flag;     // bit0 follower, bits1-2 phase code (0:+1, 1:-1, 2:0)
     double *q_val;       // pre-gate source coefficient v_src
+    uint32_t *q_count;   // [grid * warps per block] queries per warp region
+    uint32_t *blk_anti;  // [grid] anticommuting terms per sweep block
+    uint32_t *blk_q;     // [grid] queries per sweep block
     uint32_t *emit_bits; // leader-emitted flags, one bit per term (column-word layout)
     double *aux;         // pre-gate coefficients, used only for cos == 0 gates
     uint64_t q_cap;      // size of the query arrays

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,6 +50,7 @@ struct AdjointState {
     double *final_coef = nullptr;
     uint64_t n_final = 0;
     std::vector<uint64_t> stats; // [L][4] n_g, a_g, e_g, (unused) per step
+    uint32_t *w_anti = nullptr;   // [L][sweep warps] anticommuting terms per sweep warp and step
 };
 
 struct mpx_engine {
@@ -56,6 +59,7 @@ struct mpx_engine {
     Trunc tr{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
     int grid = 0;
     Store st{};
     Scratch sc{};
@@ -83,6 +87,7 @@ struct mpx_engine {
     double t_sweep_ms = 0.0, t_resolve_ms = 0.0, t_columns_ms = 0.0;
     uint64_t n_sweep = 0;
     AdjointState adj;
+    Tape fwd_tape{}; // tape fields the forward sweep fills (w_anti while recording a gradient)
     std::string err;
 };
 
@@ -102,6 +107,35 @@ mpx_status fail(mpx_engine *eng, mpx_status st, const std::string &msg) {
     return st;
 }
 
+// Device memory of every engine on a device comes from one library-owned stream-ordered pool whose
+// release threshold is unbounded: freed blocks stay mapped for the next allocation (a new engine, a
+// regrown store) instead of being unmapped and re-mapped, which for multi-GB stores costs far more than
+// the kernels. mpx_trim_device_memory hands the cached memory back.
+cudaMemPool_t engine_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    uint64_t threshold = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    pools[device] = pool;
+    return pool;
+}
+
+cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
+    return cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream);
+}
+
 uint64_t next_pow2(uint64_t x) {
     uint64_t p = 1;
     while (p < x) p <<= 1;
@@ -114,9 +148,10 @@ template <int W, int B>
 void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
     cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, Tape{});
+    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape);
     if (ev) cudaEventRecord(ev[1], e->stream);
-    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats, Tape{});
+    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
+                                                       e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
     k_columns<W><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, 0, 0, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
@@ -267,12 +302,12 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     unsigned long long *table = nullptr;
     uint32_t *cols = nullptr;
     const uint64_t tcap = next_pow2(std::max<uint64_t>(2 * cap, 64));
-    const uint64_t q_cap = cap;
+    const uint64_t q_cap = cap + (static_cast<uint64_t>(e->grid) * kWarps + 2) * 1024; // + region slack
     const uint64_t cstride = ((cap + 31) / 32 + 31) / 32 * 32; // 128-byte aligned columns
     Scratch nsc = e->sc;
     cudaError_t ce = cudaSuccess;
     auto A = [&](void **p, size_t bytes) {
-        if (ce == cudaSuccess) ce = cudaMallocAsync(p, bytes, e->stream);
+        if (ce == cudaSuccess) ce = dev_alloc(e, p, bytes);
     };
     A(reinterpret_cast<void **>(&keys), cap * W * sizeof(uint64_t));
     A(reinterpret_cast<void **>(&coef), cap * sizeof(double));
@@ -331,7 +366,7 @@ mpx_status ensure_stats(mpx_engine *eng, uint64_t n) {
     cudaFreeAsync(e->d_stats, e->stream);
     e->d_stats = nullptr;
     const uint64_t c = std::max<uint64_t>(n, 1024);
-    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&e->d_stats), c * 4 * sizeof(uint64_t), e->stream));
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_stats), c * 4 * sizeof(uint64_t)));
     e->stats_cap = c;
     return MPX_OK;
 }
@@ -381,6 +416,11 @@ void make_desc(const mpx_engine *e, const uint64_t *g, double angle, GateDesc &d
         }
     }
     d.empty = gpop == 0;
+    d.n_fold = 0;
+    for (int w = 0; w < W; ++w) d.n_fold += __builtin_popcountll(d.fold[w]);
+    int f = 0;
+    for (int w = 0; w < W && d.n_fold <= kMaxFoldCols; ++w)
+        for (uint64_t x = d.fold[w]; x != 0; x &= x - 1) d.fold_cols[f++] = static_cast<uint16_t>(64 * w + __builtin_ctzll(x));
     // The same libm calls and argument as the reference (Engine.h:555-560, FusedApply.h:45-46).
     const double c = std::cos(2.0 * angle);
     const double s = std::sin(2.0 * angle);
@@ -427,8 +467,6 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
         }
     }
     const GateFn gate = pick_gate(e->W, e->cfg.basis);
-    // Per-gate counters start from zero (the sweep of step s clears the other parity for step s+1).
-    MPX_CUDA(cudaMemsetAsync(&e->d_cnt->q_total, 0, sizeof(Counters::q_total) + sizeof(Counters::anti), e->stream));
     constexpr uint64_t kChunk = 48;
     uint64_t step = lo;
     uint64_t chunk_id = 0;
@@ -458,7 +496,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 const uint64_t n = e->h_snap[pending_slot].n;
                 s = alloc_store(e, std::max<uint64_t>(4 * n, 2 * e->st.cap), n);
                 if (s != MPX_OK) return s;
-                Counters fresh{};  // per-gate counters restart at zero
+                Counters fresh{};
                 fresh.n = n;
                 fresh.n0 = n;
                 fresh.stall = kNoStall;
@@ -531,7 +569,9 @@ void free_adjoint(mpx_engine *e) {
     for (double *p : e->adj.ck_coef)
         if (p != nullptr) cudaFreeAsync(p, e->stream);
     if (e->adj.final_coef != nullptr) cudaFreeAsync(e->adj.final_coef, e->stream);
+    if (e->adj.w_anti != nullptr) cudaFreeAsync(e->adj.w_anti, e->stream);
     e->adj = AdjointState{};
+    e->fwd_tape = Tape{};
 }
 
 // Forward pass for the gradient: resets the store to the initial operator, propagates the circuit
@@ -545,9 +585,12 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
     const uint64_t L = cd.n;
     const uint64_t K = segment_gates == 0 ? std::max<uint64_t>(L, 1) : segment_gates;
     uint64_t n = e->n_init;
+    const uint64_t n_warps = static_cast<uint64_t>(e->grid) * kWarps;
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.w_anti), std::max<uint64_t>(L, 1) * n_warps * sizeof(uint32_t)));
+    e->fwd_tape.w_anti = e->adj.w_anti;
     for (uint64_t lo = 0; lo < L; lo += K) {
         double *ck = nullptr;
-        MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double), e->stream));
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double)));
         e->adj.ck_coef.push_back(ck);
         if (n > 0) MPX_CUDA(cudaMemcpyAsync(ck, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
         e->adj.seg_lo.push_back(lo);
@@ -559,8 +602,8 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
         }
         n = e->h_cnt->n;
     }
-    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(n, 1) * sizeof(double),
-                             e->stream));
+    e->fwd_tape = Tape{};
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(n, 1) * sizeof(double)));
     if (n > 0)
         MPX_CUDA(cudaMemcpyAsync(e->adj.final_coef, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
     e->adj.n_final = n;
@@ -606,7 +649,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     uint32_t *done = nullptr;
     cudaError_t ce = cudaSuccess;
     auto A_ = [&](void **ptr, size_t bytes) {
-        if (ce == cudaSuccess) ce = cudaMallocAsync(ptr, std::max<size_t>(bytes, 16), e->stream);
+        if (ce == cudaSuccess) ce = dev_alloc(e, ptr, std::max<size_t>(bytes, 16));
     };
     A_(reinterpret_cast<void **>(&tp.u_idx), u_max * sizeof(uint32_t));
     A_(reinterpret_cast<void **>(&tp.u_val), u_max * sizeof(double));
@@ -650,6 +693,13 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     MPX_CUDA_REL(cudaMemcpyAsync(d_steps + L, p_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
     MPX_CUDA_REL(cudaMemcpyAsync(d_steps + 2 * L, n_next.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
     MPX_CUDA_REL(cudaMemsetAsync(d_cnts, 0, 2 * L * sizeof(unsigned long long), e->stream));
+    const uint32_t n_warps = static_cast<uint32_t>(e->grid) * kWarps;
+    uint64_t max_seg = 1;
+    for (size_t sg = 0; sg < S; ++sg) max_seg = std::max<uint64_t>(max_seg, (sg + 1 < S ? A.seg_lo[sg + 1] : L) - A.seg_lo[sg]);
+    uint64_t *u_off = nullptr;
+    MPX_CUDA_REL(dev_alloc(e, reinterpret_cast<void **>(&u_off), max_seg * n_warps * sizeof(uint64_t)));
+    tp.w_anti = A.w_anti;
+    tp.u_off = u_off;
     MPX_CUDA_REL(cudaMemsetAsync(grad, 0, L * sizeof(double), e->stream));
     MPX_CUDA_REL(cudaMemsetAsync(done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
     pick_adj_init(e->W, e->cfg.basis)(e, lam, nf);
@@ -665,13 +715,15 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         c.n0 = n;
         c.stall = kNoStall;
         MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+        k_undo_offsets<<<static_cast<unsigned>(hi - lo), 1024, 0, e->stream>>>(tp, n_warps, lo, u_off);
+        tp.u_off_step0 = lo;
         for (uint64_t st = lo; st < hi; ++st) replay(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), tp);
         for (uint64_t st = hi; st-- > lo;) {
             const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
             k_adj_pairs<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
             k_adj_undo<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
         }
-        e->launches += 5 * (hi - lo);
+        e->launches += 5 * (hi - lo) + 1;
         MPX_CUDA_REL(cudaGetLastError());
     }
     e->launches += 1;
@@ -688,6 +740,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     c.stall = kNoStall;
     MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
     release();
+    cudaFreeAsync(u_off, e->stream);
     MPX_CUDA(cudaStreamSynchronize(e->stream));
 #undef MPX_CUDA_REL
     if (err != 0) return fail(eng, MPX_ERR_STATE, "gradient replay diverged from the forward pass (internal error)");
@@ -729,8 +782,9 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
         return fail(nullptr, MPX_ERR_NO_DEVICE, "no CUDA device is visible; the engine has no CPU fallback");
     }
     if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, MPX_ERR_INVALID, "device ordinal out of range");
-    cudaDeviceProp prop{};
-    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10) {
+    int major = 0, sms = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cfg->device) != cudaSuccess || major != 10 ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess) {
         cudaGetLastError();
         return fail(nullptr, MPX_ERR_NO_DEVICE, "the engine is built for sm_100a (B200) only");
     }
@@ -747,7 +801,7 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     e->device = cfg->device;
     e->core = core;
     for (int w = 0; w < e->W; ++w) e->mask.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
-    e->grid = prop.multiProcessorCount * 8;
+    e->grid = sms * kSweepBlocksPerSM; // one resident wave of the sweep
     mpx_engine *eng = e;
     auto bail = [&](mpx_status st) {
         g_create_error = e->err;
@@ -758,11 +812,19 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
         e->err = "cannot create a CUDA stream";
         return bail(MPX_ERR_CUDA);
     }
+    e->pool = engine_pool(cfg->device);
+    if (e->pool == nullptr) {
+        e->err = "cannot create the device memory pool";
+        return bail(MPX_ERR_CUDA);
+    }
     cudaError_t ce = cudaMalloc(reinterpret_cast<void **>(&e->d_cnt), sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_cnt), sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.q_count), e->grid * kWarps * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_anti), e->grid * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_q), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_out), sizeof(double));
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_out), sizeof(double));
@@ -1017,6 +1079,21 @@ mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms,
     return MPX_OK;
 }
 
+mpx_status mpx_trim_device_memory(int32_t device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(nullptr, MPX_ERR_INVALID, "device ordinal out of range");
+    }
+    cudaMemPool_t pool = engine_pool(device);
+    if (pool == nullptr) return fail(nullptr, MPX_ERR_CUDA, "cannot create the device memory pool");
+    if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, MPX_ERR_CUDA, "cudaMemPoolTrimTo failed");
+    }
+    return MPX_OK;
+}
+
 const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }
 
 void mpx_destroy(mpx_engine *e) {
@@ -1034,6 +1111,9 @@ void mpx_destroy(mpx_engine *e) {
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
     for (auto &ev : e->pev) cudaEventDestroy(ev);
+    cudaFree(e->sc.q_count);
+    cudaFree(e->sc.blk_anti);
+    cudaFree(e->sc.blk_q);
     cudaFree(e->d_partial);
     cudaFree(e->d_out);
     cudaFreeHost(e->h_out);

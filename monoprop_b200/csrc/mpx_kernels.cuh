@@ -35,6 +35,23 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 }
 
 constexpr int kWarps = kBlock / 32;
+constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
+
+// Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
+// warp w of the grid scans chunks w, w + W_total, ... of 1024 terms and owns query region w.
+struct SweepGeometry {
+    uint64_t nwords, nchunks, stride;
+    uint32_t n_warps;
+};
+
+__device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
+    SweepGeometry g;
+    g.nwords = (n0 + 31) >> 5;
+    g.nchunks = (g.nwords + 31) >> 5;
+    g.n_warps = gridDim.x * kWarps;
+    g.stride = ((g.nchunks + g.n_warps - 1) / g.n_warps) * 1024;
+    return g;
+}
 
 // Fused anticommutation scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
 // Each warp owns chunks of 1024 terms (32 column words). The anticommutation bit of 32 terms at once is
@@ -42,17 +59,20 @@ constexpr int kWarps = kBlock / 32;
 // for odd |G|): only |fold| bits per term are read, not the 8W-byte key. The anticommuting terms of the
 // chunk are then spread over the 32 lanes (prefix sums + popcount bisection); each is cos-scaled, and
 // only those that pass the lower_atol gate load their key row to build the partner M^G, run the
-// structural cutoff / upper_atol rescue and the rotation phase. Emitted branches are appended to the
-// query arrays through one atomic per warp round. In REPLAY mode (a segment re-run for the gradient)
-// every anticommuting term's index and pre-gate coefficient also go to the tape's undo log.
+// structural cutoff / upper_atol rescue and the rotation phase. Emitted branches go to the warp's own
+// query region; nothing is counted through a shared global counter. With a tape, the warp's
+// anticommuting count is saved per step (forward pass of a gradient) and, in REPLAY mode, every
+// anticommuting term's index and pre-gate coefficient go to the undo log at the warp's precomputed offset.
 template <int W, int BASIS, bool REPLAY = false>
-__global__ void __launch_bounds__(kBlock) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
+__global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                    Trunc tr, Tape tp) {
     __shared__ uint32_t s_anti[kWarps][32];
     __shared__ uint32_t s_foll[kWarps][32];
     __shared__ uint32_t s_pfx[kWarps][32];
     __shared__ uint32_t s_emit[kWarps][32];
+    __shared__ uint32_t s_red[kWarps][2];
+    __shared__ uint32_t s_fold[kMaxFoldCols];
     if (cnt->stall != kNoStall) return;
     const uint64_t n0 = cnt->n;
     if (2 * n0 > st.cap) {
@@ -61,169 +81,231 @@ __global__ void __launch_bounds__(kBlock) k_sweep(Store st, Scratch sc, Counters
         if (threadIdx.x == 0) atomicMin(&cnt->stall, step);
         return;
     }
-    const uint32_t par = step & 1u;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        cnt->n0 = n0;
-        cnt->q_total[par ^ 1u] = 0;
-        cnt->anti[par ^ 1u] = 0;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n0 = n0;
     const GateDesc &gd = gates[gate];
-    if (gd.empty || n0 == 0) return;
+    const int n_fold = gd.n_fold;
+    if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    uint64_t g[W];
+    const SweepGeometry geo = sweep_geometry(n0);
+    const uint32_t wg = blockIdx.x * kWarps + warp;
+    uint32_t anti_count = 0, qcount = 0;
+    uint64_t ubase = 0;
+    if constexpr (REPLAY) ubase = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * geo.n_warps + wg];
+    if (!gd.empty && n0 != 0) {
+        uint64_t g[W];
 #pragma unroll
-    for (int w = 0; w < W; ++w) g[w] = gd.g[w];
-    const double cosv = gd.cosv, sinabs = gd.abs_sin;
-    const bool cos_zero = gd.cos_zero != 0;
-    const int gpop = gd.gpop;
-    const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(gd.pivot_col) * st.cstride;
-    const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
-    const uint64_t nwords = (n0 + 31) >> 5;
-    const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
-    uint32_t anti_count = 0;
+        for (int w = 0; w < W; ++w) g[w] = gd.g[w];
+        const double cosv = gd.cosv, sinabs = gd.abs_sin;
+        const bool cos_zero = gd.cos_zero != 0;
+        const int gpop = gd.gpop;
+        const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(gd.pivot_col) * st.cstride;
+        const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
+        const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
+        const uint64_t qbase = static_cast<uint64_t>(wg) * geo.stride;
 
-    for (uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * kWarps + warp; chunk * 32 < nwords;
-         chunk += static_cast<uint64_t>(gridDim.x) * kWarps) {
-        const uint64_t j = chunk * 32 + lane;
-        uint32_t anti = 0, foll = 0;
-        if (j < nwords) {
+        for (uint64_t chunk = wg; chunk < geo.nchunks; chunk += geo.n_warps) {
+            const uint64_t j = chunk * 32 + lane;
+            uint32_t anti = 0, foll = 0;
+            if (j < geo.nwords) {
+                if (n_fold <= kMaxFoldCols) {
+                    // all fold-column loads in flight at once
+                    uint32_t v[kMaxFoldCols];
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-                for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
-                    const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
-                    anti ^= st.cols[c * st.cstride + j];
-                }
-            }
-            if (gd.g_odd) anti ^= parity[j];
-            if (j == nwords - 1) anti &= tail;
-            foll = anti & pivot[j];
-        }
-        const int cnt_l = __popc(anti);
-        int incl = cnt_l;
+                    for (int f = 0; f < kMaxFoldCols; ++f)
+                        v[f] = f < n_fold ? st.cols[static_cast<uint64_t>(s_fold[f]) * st.cstride + j] : 0u;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        anti_count += static_cast<uint32_t>(cnt_l);
-        s_anti[warp][lane] = anti;
-        s_foll[warp][lane] = foll;
-        s_pfx[warp][lane] = static_cast<uint32_t>(incl - cnt_l);
-        s_emit[warp][lane] = 0;
-        __syncwarp();
-        for (int k = 0; k < total; k += 32) {
-            const int idx = k + lane;
-            bool emit = false, follower = false;
-            int phase = 0, owner = 0, bit = 0;
-            double v = 0.0;
-            uint64_t term = 0;
-            if (idx < total) {
-                int lo = 0, hi = 32;
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
-                    else hi = mid;
+                    for (int f = 0; f < kMaxFoldCols; ++f) anti ^= v[f];
                 }
-                owner = lo;
-                bit = nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
-                follower = (s_foll[warp][lo] >> bit) & 1u;
-                term = (chunk * 32 + static_cast<uint64_t>(lo)) * 32 + static_cast<uint64_t>(bit);
-                v = st.coef[term];
-                st.coef[term] = v * cosv;
-                if (cos_zero) sc.aux[term] = v;
-                const double av = fabs(v);
-                if (!(tr.has_lower && sinabs * av <= tr.lower)) {
-                    uint64_t m[W], p[W];
-                    load_key<W>(st.keys, term, m);
-                    int mpop = 0, ov = 0;
+                else {
 #pragma unroll
                     for (int w = 0; w < W; ++w) {
-                        p[w] = m[w] ^ g[w];
-                        mpop += __popcll(m[w]);
-                        ov += __popcll(m[w] & g[w]);
-                    }
-                    const int ppop = mpop + gpop - 2 * ov;
-                    if (keep_partner<W>(p, ppop, tr) || (tr.has_upper && sinabs * av >= tr.upper)) {
-                        emit = true;
-                        phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
+                        for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
+                            const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
+                            anti ^= st.cols[c * st.cstride + j];
+                        }
                     }
                 }
+                if (gd.g_odd) anti ^= parity[j];
+                if (j == geo.nwords - 1) anti &= tail;
+                foll = anti & pivot[j];
             }
-            if constexpr (REPLAY) {
-                const uint32_t vb = __ballot_sync(0xFFFFFFFFu, idx < total);
-                unsigned long long ub = 0;
-                if (lane == 0) ub = atomicAdd(&tp.u_cnt[step], static_cast<unsigned long long>(__popc(vb)));
-                ub = __shfl_sync(0xFFFFFFFFu, ub, 0);
+            const int cnt_l = __popc(anti);
+            int incl = cnt_l;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            s_anti[warp][lane] = anti;
+            s_foll[warp][lane] = foll;
+            s_pfx[warp][lane] = static_cast<uint32_t>(incl - cnt_l);
+            s_emit[warp][lane] = 0;
+            __syncwarp();
+            for (int k = 0; k < total; k += 32) {
+                const int idx = k + lane;
+                bool emit = false, follower = false;
+                int phase = 0, owner = 0, bit = 0;
+                double v = 0.0;
+                uint64_t term = 0;
                 if (idx < total) {
-                    const uint64_t r = tp.u_base[step] + ub + __popc(vb & lt_mask);
-                    tp.u_idx[r] = static_cast<uint32_t>(term);
-                    tp.u_val[r] = v;
+                    int lo = 0, hi = 32;
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
+                        else hi = mid;
+                    }
+                    owner = lo;
+                    bit = nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
+                    follower = (s_foll[warp][lo] >> bit) & 1u;
+                    term = (chunk * 32 + static_cast<uint64_t>(lo)) * 32 + static_cast<uint64_t>(bit);
+                    v = st.coef[term];
+                    st.coef[term] = v * cosv;
+                    if (cos_zero) sc.aux[term] = v;
+                    if constexpr (REPLAY) {
+                        const uint64_t r = ubase + anti_count + static_cast<uint64_t>(idx);
+                        tp.u_idx[r] = static_cast<uint32_t>(term);
+                        tp.u_val[r] = v;
+                    }
+                    const double av = fabs(v);
+                    if (!(tr.has_lower && sinabs * av <= tr.lower)) {
+                        uint64_t m[W], p[W];
+                        load_key<W>(st.keys, term, m);
+                        int mpop = 0, ov = 0;
+#pragma unroll
+                        for (int w = 0; w < W; ++w) {
+                            p[w] = m[w] ^ g[w];
+                            mpop += __popcll(m[w]);
+                            ov += __popcll(m[w] & g[w]);
+                        }
+                        const int ppop = mpop + gpop - 2 * ov;
+                        if (keep_partner<W>(p, ppop, tr) || (tr.has_upper && sinabs * av >= tr.upper)) {
+                            emit = true;
+                            phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
+                        }
+                    }
                 }
-            }
-            const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
-            if (eb != 0) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(&cnt->q_total[par], static_cast<unsigned long long>(__popc(eb)));
-                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
                 if (emit) {
-                    const uint64_t q = base + __popc(eb & lt_mask);
+                    const uint64_t q = qbase + qcount + __popc(eb & lt_mask);
                     sc.q_src[q] = static_cast<uint32_t>(term);
                     sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
                     sc.q_val[q] = v;
                     if (!follower) atomicOr(&s_emit[warp][owner], 1u << bit);
                 }
+                qcount += __popc(eb);
             }
+            anti_count += static_cast<uint32_t>(total);
+            __syncwarp();
+            if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][lane];
+            __syncwarp();
         }
-        __syncwarp();
-        if (j < nwords) sc.emit_bits[j] = s_emit[warp][lane];
-        __syncwarp();
     }
+    if (lane == 0) {
+        sc.q_count[wg] = qcount;
+        if (tp.w_anti != nullptr && !REPLAY) tp.w_anti[static_cast<uint64_t>(step) * geo.n_warps + wg] = anti_count;
+        s_red[warp][0] = anti_count;
+        s_red[warp][1] = qcount;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0, q = 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) anti_count += __shfl_down_sync(0xFFFFFFFFu, anti_count, o);
-    if (lane == 0 && anti_count != 0) atomicAdd(&cnt->anti[par], static_cast<unsigned long long>(anti_count));
+        for (int w = 0; w < kWarps; ++w) {
+            t += s_red[w][0];
+            q += s_red[w][1];
+        }
+        sc.blk_anti[blockIdx.x] = t;
+        sc.blk_q[blockIdx.x] = q;
+    }
 }
 
 // Partner resolve + rotation apply + append (Engine.h:364-513, FusedApply.h:32-83, MPOperator.h:269-278).
-// In REPLAY mode the keys of this gate's appends already exist (indices >= n0, inserted by the forward
-// pass): a partner found there is treated as the append it was, nothing is inserted, and every rotated
-// or appended pair goes to the tape's pair log with both pre-gate coefficients.
+// Resolve block b processes the query regions of sweep block b's warps, in block-wide rounds; appends
+// take one counter bump per round. In REPLAY mode the keys of this gate's appends already exist
+// (indices >= n0, inserted by the forward pass): a partner found there is treated as the append it was,
+// nothing is inserted, and every rotated or appended pair goes to the tape's pair log with both
+// pre-gate coefficients (one counter bump per round).
 template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                      uint64_t *__restrict__ stats, Tape tp) {
-    __shared__ uint32_t warp_miss[kWarps];
-    __shared__ unsigned long long s_base;
+    __shared__ uint32_t warp_cnt[kWarps];
+    __shared__ uint32_t s_pfx[kWarps + 1];
+    __shared__ unsigned long long s_base, s_rbase;
+    __shared__ unsigned long long s_sum[2][kWarps];
     if (cnt->stall != kNoStall) return;
-    const uint32_t par = step & 1u;
     const uint64_t n0 = cnt->n0;
-    const uint64_t total = cnt->q_total[par];
     const GateDesc &gd = gates[gate];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        stats[4 * static_cast<uint64_t>(step) + 0] = n0;
-        stats[4 * static_cast<uint64_t>(step) + 1] = cnt->anti[par];
-        stats[4 * static_cast<uint64_t>(step) + 2] = total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const SweepGeometry geo = sweep_geometry(n0);
+    if (blockIdx.x == 0) {
+        // per-gate counters for the host: n_g, a_g, e_g (fixed-order sums)
+        unsigned long long a = 0, e = 0;
+        if (!gd.empty && n0 != 0) {
+            for (uint32_t b = threadIdx.x; b < gridDim.x; b += kBlock) {
+                a += sc.blk_anti[b];
+                e += sc.blk_q[b];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xFFFFFFFFu, a, o);
+            e += __shfl_down_sync(0xFFFFFFFFu, e, o);
+        }
+        if (lane == 0) {
+            s_sum[0][warp] = a;
+            s_sum[1][warp] = e;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long ta = 0, te = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                ta += s_sum[0][w];
+                te += s_sum[1][w];
+            }
+            stats[4 * static_cast<uint64_t>(step) + 0] = n0;
+            stats[4 * static_cast<uint64_t>(step) + 1] = ta;
+            stats[4 * static_cast<uint64_t>(step) + 2] = te;
+        }
     }
+    if (gd.empty || n0 == 0) return;
+    if (threadIdx.x < kWarps) warp_cnt[threadIdx.x] = sc.q_count[blockIdx.x * kWarps + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            s_pfx[w] = acc;
+            acc += warp_cnt[w];
+        }
+        s_pfx[kWarps] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = s_pfx[kWarps];
     if (total == 0) return;
     uint64_t g[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) g[w] = gd.g[w];
     const double sinv = gd.sinv, inv_cos = gd.inv_cos;
     const bool cos_zero = gd.cos_zero != 0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt_mask = (1u << lane) - 1u;
 
-    for (uint64_t tb = static_cast<uint64_t>(blockIdx.x) * kBlock; tb < total;
-         tb += static_cast<uint64_t>(gridDim.x) * kBlock) {
-        const uint64_t q = tb + threadIdx.x;
-        bool miss = false;
+    for (uint32_t tb = 0; tb < total; tb += kBlock) {
+        const uint32_t k = tb + threadIdx.x;
+        bool miss = false, rec = false;
         uint64_t p[W];
         uint64_t pos = 0;
-        uint32_t tag = 0;
-        double v = 0.0, ph = 0.0;
-        if (q < total) {
-            const uint32_t src = sc.q_src[q];
+        uint32_t tag = 0, src = 0, tgt = 0;
+        int8_t code = 0;
+        double v = 0.0, ph = 0.0, vt = 0.0;
+        if (k < total) {
+            int r = 0;
+#pragma unroll
+            for (int w = 1; w < kWarps; ++w) r += (s_pfx[w] <= k) ? 1 : 0;
+            const uint64_t q = static_cast<uint64_t>(blockIdx.x * kWarps + r) * geo.stride + (k - s_pfx[r]);
+            src = sc.q_src[q];
             const uint8_t flag = sc.q_flag[q];
             v = sc.q_val[q];
             ph = phase_value(static_cast<uint8_t>(flag >> 1));
@@ -268,12 +350,10 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 }
                 else if (!gave_up && found >= n0) {
                     st.coef[found] = (sinv * ph) * v;
-                    const uint64_t r = tp.p_base[step] + atomicAdd(&tp.p_cnt[step], 1ULL);
-                    tp.p_src[r] = src;
-                    tp.p_tgt[r] = static_cast<uint32_t>(found);
-                    tp.p_code[r] = static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF));
-                    tp.p_vs[r] = v;
-                    tp.p_vt[r] = 0.0;
+                    rec = true;
+                    tgt = static_cast<uint32_t>(found);
+                    code = static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF));
+                    vt = 0.0;
                     gave_up = true; // handled
                 }
             }
@@ -281,35 +361,45 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 const bool follower = (flag & 1) != 0;
                 const bool leader_took_it = follower && ((sc.emit_bits[found >> 5] >> (found & 31)) & 1u);
                 if (!leader_took_it) {
-                    const double vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
+                    vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
                     st.coef[src] = __fma_rn(sinv * -ph, vt, st.coef[src]);
                     st.coef[found] = __fma_rn(sinv * ph, v, st.coef[found]);
                     if constexpr (REPLAY) {
-                        const uint64_t r = tp.p_base[step] + atomicAdd(&tp.p_cnt[step], 1ULL);
-                        tp.p_src[r] = src;
-                        tp.p_tgt[r] = static_cast<uint32_t>(found);
-                        tp.p_code[r] = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
-                        tp.p_vs[r] = v;
-                        tp.p_vt[r] = vt;
+                        rec = true;
+                        tgt = static_cast<uint32_t>(found);
+                        code = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
                     }
                 }
             }
         }
-        // Unique appends: one counter bump per block iteration.
-        const uint32_t miss_ball = __ballot_sync(0xFFFFFFFFu, miss);
-        if (lane == 0) warp_miss[warp] = __popc(miss_ball);
+        // Unique appends (forward) or pair records (replay): one counter bump per round.
+        const uint32_t ball = __ballot_sync(0xFFFFFFFFu, REPLAY ? rec : miss);
+        if (lane == 0) warp_cnt[warp] = __popc(ball);
         __syncthreads();
         uint32_t off = 0, tot = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
-            const uint32_t t = warp_miss[w];
+            const uint32_t t = warp_cnt[w];
             off += (w < warp) ? t : 0u;
             tot += t;
         }
-        if (threadIdx.x == 0 && tot > 0) s_base = atomicAdd(&cnt->n, static_cast<unsigned long long>(tot));
+        if (threadIdx.x == 0 && tot > 0) {
+            if constexpr (REPLAY) s_rbase = atomicAdd(&tp.p_cnt[step], static_cast<unsigned long long>(tot));
+            else s_base = atomicAdd(&cnt->n, static_cast<unsigned long long>(tot));
+        }
         __syncthreads();
-        if (miss) {
-            const uint64_t idx = s_base + off + __popc(miss_ball & lt_mask);
+        if constexpr (REPLAY) {
+            if (rec) {
+                const uint64_t r = tp.p_base[step] + s_rbase + off + __popc(ball & lt_mask);
+                tp.p_src[r] = src;
+                tp.p_tgt[r] = tgt;
+                tp.p_code[r] = code;
+                tp.p_vs[r] = v;
+                tp.p_vt[r] = vt;
+            }
+        }
+        else if (miss) {
+            const uint64_t idx = s_base + off + __popc(ball & lt_mask);
             store_key<W>(st.keys, idx, p);
             st.coef[idx] = (sinv * ph) * v;
             const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;

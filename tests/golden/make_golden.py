@@ -17,7 +17,8 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
   ``MajoranaOperator`` canonicalisation), with the fixture's exact energy and gradient and the reference
   engine's raw output at infinite cutoff (``cutoff = 2 n``).
 
-Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT]``.
+Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT] [--fd-full]`` (``--fd-full`` adds the slow
+finite-difference golden of the full 100-qubit circuit).
 """
 
 from __future__ import annotations
@@ -61,8 +62,13 @@ GRADS = [
     ("hubbard6x6_L300", W.hubbard6x6, 300),
     ("ising100_L600", W.ising100, 600),
     ("ising50_d2", lambda: W.ising50(2), None),
-    ("ising100", W.ising100, None),  # the full 100-qubit, 5600-angle circuit (about a minute here)
 ]
+
+# The full 100-qubit, 5600-angle circuit: the reference's analytic gradient drifts for the angles it
+# reaches last in its reverse sweep (angle 5202: -1.2165 analytic vs 4.6e-5 by finite differences of the
+# same replayed graph), so the golden is central finite differences (h = 1e-5) of its replayed graph on
+# 64 seeded angles (fd_ising100.npz; about 15 minutes on 8 cores).
+FD_FULL = ("ising100", W.ising100, 64, 1e-5, 2024)
 
 
 def digest(keys: np.ndarray, coefs: np.ndarray) -> dict:
@@ -116,6 +122,24 @@ def main(reference_root: str = "/root/reference") -> None:
         np.savez_compressed(os.path.join(HERE, f"grad_{name}.npz"), expectation=np.float64(ev), grad=grad,
                             n_layers=np.int64(n_layers), n_params=np.int64(n_params))
         print("grad", name, ev, float(np.abs(grad).max()))
+    if "--fd-full" in sys.argv:
+        name, make, count, h, seed = FD_FULL
+        wl = make()
+        eng = oracle.RefEngine(wl, partitions=8)
+        eng.propagate(build_graph=True)
+        theta = wl.params.copy()
+        idx = np.sort(np.random.default_rng(seed).choice(theta.size, size=count, replace=False))
+        fd = np.zeros(count)
+        for k, p in enumerate(idx):
+            tp, tm = theta.copy(), theta.copy()
+            tp[p] += h
+            tm[p] -= h
+            fd[k] = (eng.expectation(tp) - eng.expectation(tm)) / (2 * h)
+        ev0 = eng.expectation(theta)
+        eng.close()
+        np.savez_compressed(os.path.join(HERE, f"fd_{name}.npz"), expectation=np.float64(ev0), idx=idx, fd=fd,
+                            h=np.float64(h))
+        print("fd", name, ev0, float(np.abs(fd).max()))
     # Parameter-shift gradient of the 20-qubit line circuit from the reference's replayed graph: each
     # replayed layer is affine in (cos 2 g theta, sin 2 g theta), so E(theta + s e_p) - E(theta - s e_p)
     # with s = pi / (4 |g|) times |g| is the exact derivative of the frozen surrogate (one layer per
@@ -155,4 +179,4 @@ def main(reference_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    main(*[a for a in sys.argv[1:] if not a.startswith("--")])

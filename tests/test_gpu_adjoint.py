@@ -120,3 +120,14 @@ def test_torch_autograd():
     dp.close()
     assert abs(float(e) - ev) <= 1e-14 * max(1.0, abs(ev))
     assert np.max(np.abs(theta.grad.numpy() - grad)) <= 1e-13 * max(1.0, np.max(np.abs(grad)))
+
+
+def test_full_circuit_gradient_finite_differences():
+    """The 100-qubit, 5600-angle circuit with checkpoints every 4 circuit layers (1120 gates) against
+    central finite differences (h = 1e-5) of the reference's replayed graph on 64 seeded angles
+    (tests/golden/fd_ising100.npz): 1e-7 relative to the largest derivative."""
+    g = golden.load("fd_ising100")
+    ev, grad = value_and_grad(W.ising100(), segment_gates=4 * 280)
+    assert abs(ev - float(g["expectation"])) <= 1e-10 * max(1.0, abs(float(g["expectation"])))
+    fd = g["fd"]
+    assert np.max(np.abs(grad[g["idx"]] - fd)) <= 1e-7 * max(np.max(np.abs(fd)), np.max(np.abs(grad)))
