@@ -54,6 +54,9 @@ typedef struct {
     int32_t num_modes;     /* logical modes (qubits in the Pauli basis); kwarg logical_num_modes= */
     int32_t device;        /* CUDA device ordinal */
     uint64_t capacity_hint; /* initial term capacity; 0 = automatic. The store grows on demand. */
+    int32_t blocks_per_sm;  /* tuning: per-gate kernel grid, blocks per SM (1..4); 0 = 4 */
+    int32_t table_shift;    /* tuning: hash table slots = next_pow2(capacity << table_shift) (1..3): load
+                               factor <= 1/2, 1/4, 1/8; 0 = 1 */
 } mpx_config;
 
 typedef struct mpx_engine mpx_engine;
@@ -137,6 +140,35 @@ MPX_API mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out);
  * 12 bytes per anticommuting term-gate pair and 25 bytes per emitted sine branch. */
 MPX_API mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation);
 MPX_API mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *grad_angles);
+
+/* Batch of independent problems (observable + circuit + angles each) on one GPU. No reference
+ * counterpart: the reference runs one propagator per process (its benches loop over instances). Items
+ * are spread over opt->workers host threads, each with its own engine and CUDA stream, deepest circuit
+ * first, so the per-gate kernels of different instances share the GPU; an instance that runs out of device
+ * memory waits for another to finish and retries. Per item: <0|O|0> into *expectation, and with
+ * opt->gradient d<0|O|0>/d(angle_l) into grad_angles[n_layers] (when non-NULL). */
+typedef struct {
+    const uint64_t *obs_words; /* [n_obs][W] */
+    const double *obs_coef;
+    uint64_t n_obs;
+    double core;
+    const uint64_t *state_mask; /* [W] */
+    const uint64_t *gen_words;  /* [n_layers][W] */
+    const double *angles;       /* [n_layers], theta[map] * g */
+    uint64_t n_layers;
+    double *expectation;  /* out */
+    double *grad_angles;  /* out [n_layers], or NULL */
+    uint64_t *final_terms; /* out (store size after propagation), or NULL */
+} mpx_batch_item;
+
+typedef struct {
+    int32_t workers;        /* instances in flight (0 = 8) */
+    int32_t gradient;       /* also the adjoint gradient */
+    uint64_t segment_gates; /* gradient checkpoint interval (0 = one segment) */
+} mpx_batch_options;
+
+MPX_API mpx_status mpx_batch_run(const mpx_config *cfg, mpx_batch_item *items, uint64_t n_items,
+                                 const mpx_batch_options *opt, char *err, size_t err_len);
 
 /* Per-kernel timing. With profiling on, the sweep, resolve and column-append launches of every gate are
  * bracketed by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms)

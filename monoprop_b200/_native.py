@@ -24,7 +24,7 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
-            "mpx_destroy", "mpx_expectation_noalloc")
+            "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run")
 
 
 class MpxError(RuntimeError):
@@ -43,7 +43,7 @@ class Config(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower_atol", C.c_int32), ("lower_atol", C.c_double), ("has_upper_atol", C.c_int32),
                 ("upper_atol", C.c_double), ("num_modes", C.c_int32), ("device", C.c_int32),
-                ("capacity_hint", C.c_uint64)]
+                ("capacity_hint", C.c_uint64), ("blocks_per_sm", C.c_int32), ("table_shift", C.c_int32)]
 
 
 _lib = None
@@ -87,6 +87,7 @@ def load() -> C.CDLL:
             "mpx_destroy": (None, [vp]),
             "mpx_expectation_noalloc": (st, [C.c_int32, C.c_uint32, vp, vp, u64, vp, C.c_double, vp, vp, C.c_char_p,
                                              C.c_size_t]),
+            "mpx_batch_run": (st, [C.POINTER(Config), vp, u64, vp, C.c_char_p, C.c_size_t]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -152,11 +153,12 @@ class Engine:
     def __init__(self, *, basis: str, cutoff_type: str, cutoff: int, num_modes: int,
                  keys: np.ndarray, coefs: np.ndarray, core: float, state_mask: np.ndarray,
                  lower_atol: float | None = None, upper_atol: float | None = None, device: int = 0,
-                 capacity_hint: int = 0):
+                 capacity_hint: int = 0, blocks_per_sm: int = 0, table_shift: int = 0):
         self.lib = load()
         cfg = Config(1 if basis == "pauli" else 0, 1 if cutoff_type == "support" else 0, int(cutoff),
                      int(lower_atol is not None), float(lower_atol or 0.0), int(upper_atol is not None),
-                     float(upper_atol or 0.0), int(num_modes), int(device), int(capacity_hint))
+                     float(upper_atol or 0.0), int(num_modes), int(device), int(capacity_hint),
+                     int(blocks_per_sm), int(table_shift))
         self.words = (int(num_modes) + 31) // 32
         k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, self.words)
         c = np.ascontiguousarray(coefs, dtype=np.float64).reshape(-1)

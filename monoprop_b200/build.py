@@ -35,7 +35,7 @@ def _sources(exts: tuple[str, ...]) -> list[str]:
 
 
 def build_engine(force: bool = False, verbose: bool = False) -> str:
-    cu = [os.path.join(CSRC, "mpx_engine.cu"), os.path.join(CSRC, "mpx_noalloc.cu")]
+    cu = [os.path.join(CSRC, "mpx_engine.cu"), os.path.join(CSRC, "mpx_noalloc.cu"), os.path.join(CSRC, "mpx_batch.cu")]
     deps = _sources((".cu", ".cuh", ".h")) + [os.path.join(ROOT, "include", "mpx.h")]
     if force or _stale(LIB, deps):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",

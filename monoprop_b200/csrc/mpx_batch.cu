@@ -1,0 +1,148 @@
+// mpx_batch.cu -- many independent propagation problems (observables, parameter sets, circuits of uneven
+// depth) on one GPU at once.
+//
+// The reference runs one propagator per process. Here a batch is spread over `workers` host threads,
+// each driving its own engine and CUDA stream, so the per-gate kernels of different instances run
+// concurrently on the GPU: small or shallow instances, which cannot fill 148 SMs alone, share the
+// machine, and the deepest instances start first (longest-processing-time order) so the tail is short.
+// Device memory is bounded by admission: an instance that fails to allocate waits until another worker
+// finishes and retries; only an instance that cannot fit on an otherwise idle GPU is an error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mpx.h"
+
+namespace {
+
+struct BatchState {
+    std::mutex mu;
+    std::condition_variable cv;
+    int in_flight = 0;
+    uint64_t completions = 0;
+    std::atomic<uint64_t> next{0};
+    std::atomic<bool> failed{false};
+    mpx_status status = MPX_OK;
+    std::string error;
+};
+
+// One instance on a fresh engine (the device memory pool makes engine creation cheap).
+mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_options &opt, std::string &err) {
+    mpx_engine *e = nullptr;
+    mpx_status s = mpx_create(&cfg, it.obs_words, it.obs_coef, it.n_obs, it.core, it.state_mask, &e);
+    if (s != MPX_OK) {
+        err = mpx_last_error(nullptr);
+        return s;
+    }
+    mpx_circuit *c = nullptr;
+    s = mpx_circuit_upload(e, it.gen_words, it.angles, it.n_layers, &c);
+    if (s == MPX_OK) {
+        if (opt.gradient && it.grad_angles != nullptr) {
+            s = mpx_adjoint_forward(e, c, opt.segment_gates, it.expectation);
+            if (s == MPX_OK) s = mpx_adjoint_backward(e, c, it.grad_angles);
+        }
+        else {
+            s = mpx_propagate_circuit(e, c);
+            if (s == MPX_OK) s = mpx_expectation(e, it.expectation);
+        }
+        if (s == MPX_OK && it.final_terms != nullptr) s = mpx_size(e, it.final_terms);
+    }
+    if (s != MPX_OK) err = mpx_last_error(e);
+    mpx_circuit_destroy(c);
+    mpx_destroy(e);
+    return s;
+}
+
+void worker(const mpx_config &cfg, mpx_batch_item *items, const std::vector<uint64_t> &order,
+            const mpx_batch_options &opt, BatchState &bs) {
+    if (cudaSetDevice(cfg.device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (;;) {
+        if (bs.failed.load()) return;
+        const uint64_t k = bs.next.fetch_add(1);
+        if (k >= order.size()) return;
+        mpx_batch_item &it = items[order[k]];
+        for (;;) {
+            uint64_t seen;
+            {
+                std::lock_guard<std::mutex> lock(bs.mu);
+                ++bs.in_flight;
+                seen = bs.completions;
+            }
+            std::string err;
+            const mpx_status s = run_one(cfg, it, opt, err);
+            int others;
+            {
+                std::lock_guard<std::mutex> lock(bs.mu);
+                --bs.in_flight;
+                ++bs.completions;
+                others = bs.in_flight;
+            }
+            bs.cv.notify_all();
+            if (s == MPX_OK) break;
+            if (s == MPX_ERR_NOMEM && others > 0) {
+                // memory admission: retry once some other instance has released its store
+                std::unique_lock<std::mutex> lock(bs.mu);
+                bs.cv.wait(lock, [&] { return bs.completions > seen + 1 || bs.in_flight == 0 || bs.failed.load(); });
+                continue;
+            }
+            std::lock_guard<std::mutex> lock(bs.mu);
+            if (!bs.failed.exchange(true)) {
+                bs.status = s;
+                bs.error = "instance " + std::to_string(order[k]) + ": " + err;
+            }
+            bs.cv.notify_all();
+            return;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+MPX_API mpx_status mpx_batch_run(const mpx_config *cfg, mpx_batch_item *items, uint64_t n_items,
+                                 const mpx_batch_options *opt, char *err, size_t err_len) {
+    auto report = [&](mpx_status st, const std::string &msg) {
+        if (err != nullptr && err_len > 0) {
+            std::strncpy(err, msg.c_str(), err_len - 1);
+            err[err_len - 1] = '\0';
+        }
+        return st;
+    };
+    if (cfg == nullptr || opt == nullptr || (n_items > 0 && items == nullptr))
+        return report(MPX_ERR_INVALID, "NULL argument");
+    for (uint64_t i = 0; i < n_items; ++i) {
+        const mpx_batch_item &it = items[i];
+        if (it.expectation == nullptr || (it.n_layers > 0 && (it.gen_words == nullptr || it.angles == nullptr)) ||
+            (it.n_obs > 0 && (it.obs_words == nullptr || it.obs_coef == nullptr)))
+            return report(MPX_ERR_INVALID, "batch item " + std::to_string(i) + " has a NULL buffer");
+    }
+    // deepest first: the longest instances start early, short ones fill in around them
+    std::vector<uint64_t> order(n_items);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint64_t a, uint64_t b) { return items[a].n_layers > items[b].n_layers; });
+    const int workers = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(opt->workers > 0 ? opt->workers : 8,
+                                                                                 std::max<uint64_t>(n_items, 1))));
+    BatchState bs;
+    std::vector<std::thread> pool;
+    pool.reserve(workers);
+    for (int w = 0; w < workers; ++w) pool.emplace_back(worker, std::cref(*cfg), items, std::cref(order), std::cref(*opt),
+                                                       std::ref(bs));
+    for (auto &t : pool) t.join();
+    if (bs.failed.load()) return report(bs.status, bs.error);
+    return MPX_OK;
+}
+
+}  // extern "C"

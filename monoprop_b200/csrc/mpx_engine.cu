@@ -35,6 +35,7 @@ struct mpx_circuit {
     std::vector<uint64_t> words; // host copy of the generators, for mpx_circuit_set_angles
     int W = 1;
     int device = 0;
+    bool any_cos_zero = false; // some gate has cos(2 angle) == 0 exactly (needs the pre-gate copy `aux`)
 };
 using CircuitDev = mpx_circuit;
 
@@ -61,6 +62,8 @@ struct mpx_engine {
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
     int grid = 0;
+    int table_shift = 1;
+    bool aux_on = false; // the store carries `aux` (only circuits with an exact cos == 0 gate need it)
     Store st{};
     Scratch sc{};
     Counters *d_cnt = nullptr;
@@ -136,6 +139,10 @@ cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
     return cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream);
 }
 
+void dev_free(mpx_engine *e, void *ptr) {
+    if (ptr != nullptr) cudaFreeAsync(ptr, e->stream);
+}
+
 uint64_t next_pow2(uint64_t x) {
     uint64_t p = 1;
     while (p < x) p <<= 1;
@@ -153,7 +160,6 @@ void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t 
     k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
                                                        e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    k_columns<W><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, 0, 0, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
 }
 
@@ -301,7 +307,7 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     double *coef = nullptr;
     unsigned long long *table = nullptr;
     uint32_t *cols = nullptr;
-    const uint64_t tcap = next_pow2(std::max<uint64_t>(2 * cap, 64));
+    const uint64_t tcap = next_pow2(std::max<uint64_t>(cap << e->table_shift, 64));
     const uint64_t q_cap = cap + (static_cast<uint64_t>(e->grid) * kWarps + 2) * 1024; // + region slack
     const uint64_t cstride = ((cap + 31) / 32 + 31) / 32 * 32; // 128-byte aligned columns
     Scratch nsc = e->sc;
@@ -317,17 +323,18 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     A(reinterpret_cast<void **>(&nsc.q_flag), q_cap * sizeof(uint8_t));
     A(reinterpret_cast<void **>(&nsc.q_val), q_cap * sizeof(double));
     A(reinterpret_cast<void **>(&nsc.emit_bits), cstride * sizeof(uint32_t));
-    A(reinterpret_cast<void **>(&nsc.aux), cap * sizeof(double));
+    if (e->aux_on) A(reinterpret_cast<void **>(&nsc.aux), cap * sizeof(double));
+    else nsc.aux = nullptr;
     if (ce != cudaSuccess) {
-        cudaFreeAsync(keys, e->stream);
-        cudaFreeAsync(coef, e->stream);
-        cudaFreeAsync(table, e->stream);
-        cudaFreeAsync(cols, e->stream);
-        cudaFreeAsync(nsc.q_src == e->sc.q_src ? nullptr : nsc.q_src, e->stream);
-        cudaFreeAsync(nsc.q_flag == e->sc.q_flag ? nullptr : nsc.q_flag, e->stream);
-        cudaFreeAsync(nsc.q_val == e->sc.q_val ? nullptr : nsc.q_val, e->stream);
-        cudaFreeAsync(nsc.emit_bits == e->sc.emit_bits ? nullptr : nsc.emit_bits, e->stream);
-        cudaFreeAsync(nsc.aux == e->sc.aux ? nullptr : nsc.aux, e->stream);
+        dev_free(e, keys);
+        dev_free(e, coef);
+        dev_free(e, table);
+        dev_free(e, cols);
+        dev_free(e, nsc.q_src == e->sc.q_src ? nullptr : nsc.q_src);
+        dev_free(e, nsc.q_flag == e->sc.q_flag ? nullptr : nsc.q_flag);
+        dev_free(e, nsc.q_val == e->sc.q_val ? nullptr : nsc.q_val);
+        dev_free(e, nsc.emit_bits == e->sc.emit_bits ? nullptr : nsc.emit_bits);
+        dev_free(e, nsc.aux == e->sc.aux ? nullptr : nsc.aux);
         cudaGetLastError();
         return fail(eng, MPX_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(ce));
     }
@@ -335,15 +342,15 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
         MPX_CUDA(cudaMemcpyAsync(keys, e->st.keys, n_keep * W * sizeof(uint64_t), cudaMemcpyDeviceToDevice, e->stream));
         MPX_CUDA(cudaMemcpyAsync(coef, e->st.coef, n_keep * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
     }
-    cudaFreeAsync(e->st.keys, e->stream);
-    cudaFreeAsync(e->st.coef, e->stream);
-    cudaFreeAsync(e->st.table, e->stream);
-    cudaFreeAsync(e->st.cols, e->stream);
-    cudaFreeAsync(e->sc.q_src, e->stream);
-    cudaFreeAsync(e->sc.q_flag, e->stream);
-    cudaFreeAsync(e->sc.q_val, e->stream);
-    cudaFreeAsync(e->sc.emit_bits, e->stream);
-    cudaFreeAsync(e->sc.aux, e->stream);
+    dev_free(e, e->st.keys);
+    dev_free(e, e->st.coef);
+    dev_free(e, e->st.table);
+    dev_free(e, e->st.cols);
+    dev_free(e, e->sc.q_src);
+    dev_free(e, e->sc.q_flag);
+    dev_free(e, e->sc.q_val);
+    dev_free(e, e->sc.emit_bits);
+    dev_free(e, e->sc.aux);
     e->st.keys = keys;
     e->st.coef = coef;
     e->st.table = table;
@@ -354,6 +361,8 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     nsc.q_cap = q_cap;
     e->sc = nsc;
     MPX_CUDA(cudaMemsetAsync(table, 0xFF, tcap * sizeof(unsigned long long), e->stream));
+    // column bits of terms not yet stored must be zero (appends OR theirs in)
+    MPX_CUDA(cudaMemsetAsync(cols, 0, (64 * W + 1) * cstride * sizeof(uint32_t), e->stream));
     pick_build(W)(e, 0, n_keep);
     e->launches += n_keep > 0 ? 2 : 0;
     MPX_CUDA(cudaGetLastError());
@@ -363,7 +372,7 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
 mpx_status ensure_stats(mpx_engine *eng, uint64_t n) {
     mpx_engine *e = eng;
     if (n <= e->stats_cap) return MPX_OK;
-    cudaFreeAsync(e->d_stats, e->stream);
+    dev_free(e, e->d_stats);
     e->d_stats = nullptr;
     const uint64_t c = std::max<uint64_t>(n, 1024);
     MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_stats), c * 4 * sizeof(uint64_t)));
@@ -444,6 +453,8 @@ mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const doub
     MPX_CUDA(cudaStreamSynchronize(e->stream)); // h goes out of scope
     cd.n = n;
     cd.W = e->W;
+    cd.any_cos_zero = false;
+    for (const GateDesc &g : h) cd.any_cos_zero = cd.any_cos_zero || g.cos_zero;
     cd.device = e->device;
     cd.words.assign(gen_words, gen_words + n * e->W);
     return MPX_OK;
@@ -459,6 +470,10 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     if (L == 0) return MPX_OK;
     mpx_status s = ensure_stats(e, L);
     if (s != MPX_OK) return s;
+    if (cd.any_cos_zero && !e->aux_on) {
+        e->aux_on = true;
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->sc.aux), e->st.cap * sizeof(double)));
+    }
     if (e->profile) {
         while (e->pev.size() < 4 * L) {
             cudaEvent_t ev = nullptr;
@@ -479,7 +494,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             for (uint64_t st = step; st < stop; ++st) {
                 gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
             }
-            e->launches += 3 * (stop - step);
+            e->launches += 2 * (stop - step);
             MPX_CUDA(cudaGetLastError());
             const uint64_t slot = chunk_id & 1;
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[slot], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
@@ -494,7 +509,8 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 MPX_CUDA(cudaStreamSynchronize(e->stream));
                 const uint64_t at = snap.stall;
                 const uint64_t n = e->h_snap[pending_slot].n;
-                s = alloc_store(e, std::max<uint64_t>(4 * n, 2 * e->st.cap), n);
+                // room for the worst case of the stalled gate (2n) with headroom, at least doubling
+                s = alloc_store(e, std::max<uint64_t>(3 * n, 2 * e->st.cap), n);
                 if (s != MPX_OK) return s;
                 Counters fresh{};
                 fresh.n = n;
@@ -550,6 +566,13 @@ mpx_status load_initial(mpx_engine *eng) {
                                  e->stream));
     }
     MPX_CUDA(cudaMemsetAsync(e->st.table, 0xFF, (e->st.tmask + 1) * sizeof(unsigned long long), e->stream));
+    {
+        // clear the column bits of the terms the previous propagation appended
+        const uint64_t w0 = (e->n_init + 31) / 32;
+        if (w0 < e->st.cstride)
+            MPX_CUDA(cudaMemset2DAsync(e->st.cols + w0, e->st.cstride * sizeof(uint32_t), 0,
+                                       (e->st.cstride - w0) * sizeof(uint32_t), 64 * W + 1, e->stream));
+    }
     pick_build(W)(e, 0, e->n_init);
     e->launches += e->n_init > 0 ? 2 : 0;
     Counters c{};
@@ -567,9 +590,9 @@ mpx_status load_initial(mpx_engine *eng) {
 
 void free_adjoint(mpx_engine *e) {
     for (double *p : e->adj.ck_coef)
-        if (p != nullptr) cudaFreeAsync(p, e->stream);
-    if (e->adj.final_coef != nullptr) cudaFreeAsync(e->adj.final_coef, e->stream);
-    if (e->adj.w_anti != nullptr) cudaFreeAsync(e->adj.w_anti, e->stream);
+        dev_free(e, p);
+    dev_free(e, e->adj.final_coef);
+    dev_free(e, e->adj.w_anti);
     e->adj = AdjointState{};
     e->fwd_tape = Tape{};
 }
@@ -668,7 +691,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
                           static_cast<void *>(tp.p_tgt), static_cast<void *>(tp.p_code), static_cast<void *>(tp.p_vs),
                           static_cast<void *>(tp.p_vt), static_cast<void *>(d_steps), static_cast<void *>(d_cnts),
                           static_cast<void *>(lam), static_cast<void *>(grad), static_cast<void *>(done)})
-            if (ptr != nullptr) cudaFreeAsync(ptr, e->stream);
+            dev_free(e, ptr);
     };
     if (ce != cudaSuccess) {
         cudaGetLastError();
@@ -740,7 +763,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     c.stall = kNoStall;
     MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
     release();
-    cudaFreeAsync(u_off, e->stream);
+    dev_free(e, u_off);
     MPX_CUDA(cudaStreamSynchronize(e->stream));
 #undef MPX_CUDA_REL
     if (err != 0) return fail(eng, MPX_ERR_STATE, "gradient replay diverged from the forward pass (internal error)");
@@ -801,7 +824,9 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     e->device = cfg->device;
     e->core = core;
     for (int w = 0; w < e->W; ++w) e->mask.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
-    e->grid = sms * kSweepBlocksPerSM; // one resident wave of the sweep
+    const int bps = cfg->blocks_per_sm > 0 ? std::min(cfg->blocks_per_sm, kSweepBlocksPerSM) : kSweepBlocksPerSM;
+    e->grid = sms * bps; // one resident wave of the sweep
+    e->table_shift = cfg->table_shift > 0 ? std::min(cfg->table_shift, 3) : 1;
     mpx_engine *eng = e;
     auto bail = [&](mpx_status st) {
         g_create_error = e->err;
@@ -859,7 +884,7 @@ mpx_status mpx_propagate(mpx_engine *e, const uint64_t *gen_words, const double 
     CircuitDev cd;
     mpx_status s = upload_circuit(e, gen_words, angles, n_layers, cd);
     if (s == MPX_OK) s = run_circuit(e, cd);
-    cudaFreeAsync(cd.d_desc, e->stream);
+    dev_free(e, cd.d_desc);
     cudaStreamSynchronize(e->stream);
     cd.d_desc = nullptr;
     return s;
@@ -890,6 +915,8 @@ mpx_status mpx_circuit_set_angles(mpx_engine *e, mpx_circuit *c, const double *a
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
     std::vector<GateDesc> h(c->n);
     for (uint64_t l = 0; l < c->n; ++l) make_desc(e, c->words.data() + l * e->W, angles[l], h[l]);
+    c->any_cos_zero = false;
+    for (const GateDesc &g : h) c->any_cos_zero = c->any_cos_zero || g.cos_zero;
     MPX_CUDA(cudaSetDevice(e->device));
     if (c->n > 0) {
         MPX_CUDA(cudaMemcpyAsync(c->d_desc, h.data(), c->n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));

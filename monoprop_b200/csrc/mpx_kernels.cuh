@@ -1,13 +1,14 @@
 // mpx_kernels.cuh -- the per-gate kernels of the B200 propagation engine (sm_100a).
 //
-// One Heisenberg gate = three launches over the device term store:
+// One Heisenberg gate = two launches over the device term store:
 //   k_sweep   -- anticommutation test from the generator's bit-columns (|fold| bits per term), fused cos
 //                scaling of the anticommuting coefficients, lower_atol / structural-cutoff / upper_atol
 //                emit gate, rotation phase, leader/follower class; compacts the emitted sine branches into
 //                the query arrays and writes the leader-emitted bitmap.
 //   k_resolve -- one thread per emitted branch: open-addressing lookup of the partner M^G, the
 //                leader/follower rule, the rotation of the pair, or the unique append of the missing partner.
-//   k_columns -- adds the appended terms to the bit-columns.
+//              The appended terms' bit-columns are OR-ed in by the same kernel.
+//   k_columns -- (re)builds the bit-columns of a range of stored terms (construction, growth, reset).
 // Every coefficient slot is written by exactly one thread per gate (the sine partner map M -> M^G is
 // injective), so no coefficient atomics are needed (layer_build/FusedApply.h:54-56).
 #pragma once
@@ -36,6 +37,7 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
+constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
 // warp w of the grid scans chunks w, w + W_total, ... of 1024 terms and owns query region w.
@@ -94,9 +96,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     uint64_t ubase = 0;
     if constexpr (REPLAY) ubase = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * geo.n_warps + wg];
     if (!gd.empty && n0 != 0) {
-        uint64_t g[W];
-#pragma unroll
-        for (int w = 0; w < W; ++w) g[w] = gd.g[w];
         const double cosv = gd.cosv, sinabs = gd.abs_sin;
         const bool cos_zero = gd.cos_zero != 0;
         const int gpop = gd.gpop;
@@ -144,58 +143,74 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
             s_pfx[warp][lane] = static_cast<uint32_t>(incl - cnt_l);
             s_emit[warp][lane] = 0;
             __syncwarp();
-            for (int k = 0; k < total; k += 32) {
-                const int idx = k + lane;
-                bool emit = false, follower = false;
-                int phase = 0, owner = 0, bit = 0;
-                double v = 0.0;
-                uint64_t term = 0;
-                if (idx < total) {
-                    int lo = 0, hi = 32;
-                    while (hi - lo > 1) {
-                        const int mid = (lo + hi) >> 1;
-                        if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
-                        else hi = mid;
-                    }
-                    owner = lo;
-                    bit = nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
-                    follower = (s_foll[warp][lo] >> bit) & 1u;
-                    term = (chunk * 32 + static_cast<uint64_t>(lo)) * 32 + static_cast<uint64_t>(bit);
-                    v = st.coef[term];
-                    st.coef[term] = v * cosv;
-                    if (cos_zero) sc.aux[term] = v;
-                    if constexpr (REPLAY) {
-                        const uint64_t r = ubase + anti_count + static_cast<uint64_t>(idx);
-                        tp.u_idx[r] = static_cast<uint32_t>(term);
-                        tp.u_val[r] = v;
-                    }
-                    const double av = fabs(v);
-                    if (!(tr.has_lower && sinabs * av <= tr.lower)) {
-                        uint64_t m[W], p[W];
-                        load_key<W>(st.keys, term, m);
-                        int mpop = 0, ov = 0;
+            // Rounds of up to 32 * kPrefetch anticommuting terms: every lane first issues the coefficient
+            // loads of its kPrefetch terms (independent random accesses in flight together), then
+            // processes them one by one.
+            for (int k = 0; k < total; k += 32 * kPrefetch) {
+                int loc[kPrefetch];
+                double vv[kPrefetch];
 #pragma unroll
-                        for (int w = 0; w < W; ++w) {
-                            p[w] = m[w] ^ g[w];
-                            mpop += __popcll(m[w]);
-                            ov += __popcll(m[w] & g[w]);
+                for (int r = 0; r < kPrefetch; ++r) {
+                    const int idx = k + 32 * r + lane;
+                    loc[r] = -1;
+                    vv[r] = 0.0;
+                    if (idx < total) {
+                        int lo = 0, hi = 32;
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
+                            else hi = mid;
                         }
-                        const int ppop = mpop + gpop - 2 * ov;
-                        if (keep_partner<W>(p, ppop, tr) || (tr.has_upper && sinabs * av >= tr.upper)) {
-                            emit = true;
-                            phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
-                        }
+                        loc[r] = lo * 32 + nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
+                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(loc[r])];
                     }
                 }
-                const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
-                if (emit) {
-                    const uint64_t q = qbase + qcount + __popc(eb & lt_mask);
-                    sc.q_src[q] = static_cast<uint32_t>(term);
-                    sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
-                    sc.q_val[q] = v;
-                    if (!follower) atomicOr(&s_emit[warp][owner], 1u << bit);
+#pragma unroll
+                for (int r = 0; r < kPrefetch; ++r) {
+                    if (k + 32 * r >= total) break; // warp-uniform
+                    const int l = loc[r];
+                    const double v = vv[r];
+                    const uint64_t term = chunk * 1024 + static_cast<uint64_t>(l < 0 ? 0 : l);
+                    bool emit = false, follower = false;
+                    int phase = 0;
+                    if (l >= 0) {
+                        follower = (s_foll[warp][l >> 5] >> (l & 31)) & 1u;
+                        st.coef[term] = v * cosv;
+                        if (cos_zero) sc.aux[term] = v;
+                        if constexpr (REPLAY) {
+                            const uint64_t rr = ubase + anti_count + static_cast<uint64_t>(k + 32 * r + lane);
+                            tp.u_idx[rr] = static_cast<uint32_t>(term);
+                            tp.u_val[rr] = v;
+                        }
+                        const double av = fabs(v);
+                        if (!(tr.has_lower && sinabs * av <= tr.lower)) {
+                            uint64_t m[W], p[W];
+                            load_key<W>(st.keys, term, m);
+                            int mpop = 0, ov = 0;
+#pragma unroll
+                            for (int w = 0; w < W; ++w) {
+                                const uint64_t gw = gd.g[w];
+                                p[w] = m[w] ^ gw;
+                                mpop += __popcll(m[w]);
+                                ov += __popcll(m[w] & gw);
+                            }
+                            const int ppop = mpop + gpop - 2 * ov;
+                            if (keep_partner<W>(p, ppop, tr) || (tr.has_upper && sinabs * av >= tr.upper)) {
+                                emit = true;
+                                phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
+                            }
+                        }
+                    }
+                    const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
+                    if (emit) {
+                        const uint64_t q = qbase + qcount + __popc(eb & lt_mask);
+                        sc.q_src[q] = static_cast<uint32_t>(term);
+                        sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
+                        sc.q_val[q] = v;
+                        if (!follower) atomicOr(&s_emit[warp][l >> 5], 1u << (l & 31));
+                    }
+                    qcount += __popc(eb);
                 }
-                qcount += __popc(eb);
             }
             anti_count += static_cast<uint32_t>(total);
             __syncwarp();
@@ -398,19 +413,58 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 tp.p_vt[r] = vt;
             }
         }
-        else if (miss) {
-            const uint64_t idx = s_base + off + __popc(ball & lt_mask);
-            store_key<W>(st.keys, idx, p);
-            st.coef[idx] = (sinv * ph) * v;
-            const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
-            for (uint64_t probes = 0;; ++probes) {
-                if (probes > st.tmask) {
-                    atomicOr(&cnt->err, 2u);
-                    break;
+        else {
+            const uint64_t first = s_base + off; // this warp's appends are [first, first + popc(ball))
+            const uint64_t idx = first + __popc(ball & lt_mask);
+            if (miss) {
+                store_key<W>(st.keys, idx, p);
+                st.coef[idx] = (sinv * ph) * v;
+                const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
+                for (uint64_t probes = 0;; ++probes) {
+                    if (probes > st.tmask) {
+                        atomicOr(&cnt->err, 2u);
+                        break;
+                    }
+                    const unsigned long long old = atomicCAS(&st.table[pos], kEmptySlot, mine);
+                    if (old == kEmptySlot) break;
+                    pos = (pos + 1) & st.tmask;
                 }
-                const unsigned long long old = atomicCAS(&st.table[pos], kEmptySlot, mine);
-                if (old == kEmptySlot) break;
-                pos = (pos + 1) & st.tmask;
+            }
+            if (ball != 0) {
+                // Bit-columns of the appended terms (InvertedIndex::append_rows, InvertedIndex.h:178-193).
+                // The warp's indices are consecutive, so they touch at most two column words: per column
+                // the lanes' bits are combined by a warp reduction and OR-ed into each word once. Column
+                // bits of terms not yet appended are zero, so OR is enough.
+                const uint64_t j0 = first >> 5;
+                const uint32_t mybit = miss ? (1u << (idx & 31)) : 0u;
+                const bool upper = miss && ((idx >> 5) != j0);
+                int pop = 0;
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    const uint64_t pk = miss ? p[w] : 0ULL;
+                    pop += __popcll(pk);
+                    uint64_t u = (static_cast<uint64_t>(__reduce_or_sync(0xFFFFFFFFu, static_cast<uint32_t>(pk >> 32)))
+                                  << 32) |
+                                 __reduce_or_sync(0xFFFFFFFFu, static_cast<uint32_t>(pk));
+                    for (; u != 0; u &= u - 1) {
+                        const int b = __ffsll(static_cast<long long>(u)) - 1;
+                        const bool has = (pk >> b) & 1ULL;
+                        const uint32_t r0 = __reduce_or_sync(0xFFFFFFFFu, (has && !upper) ? mybit : 0u);
+                        const uint32_t r1 = __reduce_or_sync(0xFFFFFFFFu, (has && upper) ? mybit : 0u);
+                        if (lane == 0) {
+                            uint32_t *col = st.cols + static_cast<uint64_t>(64 * w + b) * st.cstride;
+                            if (r0) atomicOr(col + j0, r0);
+                            if (r1) atomicOr(col + j0 + 1, r1);
+                        }
+                    }
+                }
+                const uint32_t r0 = __reduce_or_sync(0xFFFFFFFFu, ((pop & 1) && !upper) ? mybit : 0u);
+                const uint32_t r1 = __reduce_or_sync(0xFFFFFFFFu, ((pop & 1) && upper) ? mybit : 0u);
+                if (lane == 0) {
+                    uint32_t *col = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
+                    if (r0) atomicOr(col + j0, r0);
+                    if (r1) atomicOr(col + j0 + 1, r1);
+                }
             }
         }
         __syncthreads();
@@ -419,8 +473,8 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
 
 // Writes the bit-columns of terms [lo, hi): one warp per 32-term column word, one ballot per key bit.
 // A word that starts below lo already holds valid bits for the terms below lo (and zeros above) and is
-// OR-ed; every other word is assigned whole, so no clearing is ever needed. With from_counters the range
-// is the current gate's appends [n0, n).
+// OR-ed; every other word is assigned whole (zeros above hi included). With from_counters the range is
+// the current gate's appends [n0, n).
 template <int W>
 __global__ void __launch_bounds__(kBlock) k_columns(Store st, const Counters *__restrict__ cnt, uint64_t lo,
                                                      uint64_t hi, int from_counters) {

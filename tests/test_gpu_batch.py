@@ -1,0 +1,60 @@
+"""Batches of independent problems (mpx_batch_run) and the batch autotuner.
+
+Every instance of a batch must give what it gives alone: <O> against the oracle (1e-10 relative), the
+store size against the oracle's, and with gradients the single-instance adjoint's gradient, whatever
+the concurrency and tuning knobs.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from monoprop_b200 import workloads as W
+from monoprop_b200.autograd import DifferentiablePropagation
+from monoprop_b200.batch import Autotuner, BatchConfig, run_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch(n=12, seed=3):
+    rng = np.random.default_rng(seed)
+    return [W.ising50(int(d), seed=100 + i, observable_qubit=int(q))
+            for i, (d, q) in enumerate(zip(rng.integers(1, 4, size=n), rng.integers(0, 50, size=n)))]
+
+
+@pytest.mark.parametrize("cfg", [BatchConfig(1, 0, 0), BatchConfig(8, 2, 2), BatchConfig(16, 4, 1)])
+def test_batch_matches_single_instances(cfg):
+    batch = small_batch()
+    r = run_batch(batch, cfg)
+    for wl, ev, n in zip(batch, r.expectations, r.final_terms):
+        ref = oracle.run_port(wl)
+        assert abs(ev - ref.expectation) <= 1e-10 * max(1.0, abs(ref.expectation))
+        assert int(n) == ref.keys.shape[0]
+
+
+def test_batch_gradients_match_single_instance():
+    batch = small_batch(6, seed=9)
+    r = run_batch(batch, BatchConfig(4), gradient=True, segment_gates=135)
+    for wl, ev, g in zip(batch, r.expectations, r.grads):
+        dp = DifferentiablePropagation(wl, segment_gates=135)
+        ev1 = dp.forward_value(wl.params)
+        ga = dp.engine.adjoint_backward(dp.circuit)
+        dp.close()
+        assert abs(ev - ev1) <= 1e-13 * max(1.0, abs(ev1))
+        assert np.max(np.abs(g - ga)) <= 1e-12 * max(1.0, np.max(np.abs(ga)))
+
+
+def test_autotuner_picks_a_measured_configuration(tmp_path):
+    batch = small_batch(16, seed=5)
+    tuner = Autotuner(cache_path=str(tmp_path / "tune.json"), sample=6)
+    best, entry = tuner.tune(batch)
+    assert len(entry["table"]) == len(Autotuner.WORKERS) * len(Autotuner.BLOCKS_PER_SM) * len(Autotuner.TABLE_SHIFT)
+    assert min(row["seconds"] for row in entry["table"]) == min(
+        row["seconds"] for row in entry["table"] if row["workers"] == best.workers
+        and row["blocks_per_sm"] == best.blocks_per_sm and row["table_shift"] == best.table_shift)
+    again, _ = tuner.tune(batch)  # served from the cache
+    assert again == best
+    r = run_batch(batch, best)
+    for wl, ev in zip(batch, r.expectations):
+        ref = oracle.run_port(wl)
+        assert abs(ev - ref.expectation) <= 1e-10 * max(1.0, abs(ref.expectation))
