@@ -117,6 +117,18 @@ def _dist():
     return rank, ws, local, dist
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's ``value`` (timings are reported as the slowest rank's); every rank
+    takes part in the same collective."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _cpu_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -265,11 +277,7 @@ def main() -> None:
         sweep_ms.append(s_ms)
         resolve_ms.append(r_ms)
         columns_ms.append(c_ms)
-    total_ms = sum(ms)
-    if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(ms), dist, dev)
     ms_per_step = total_ms / args.steps
     value = updates * world / (ms_per_step * 1e-3)
     ev_dev = eng.expectation()
@@ -293,11 +301,7 @@ def main() -> None:
             b.synchronize()
             if i > 0:
                 g_ms.append(a.elapsed_time(b))
-        g_total = sum(g_ms)
-        if dist is not None:
-            t = torch.tensor([g_total], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            g_total = float(t.item())
+        g_total = max_over_ranks(sum(g_ms), dist, dev)
         g_per = g_total / len(g_ms)
         grad_line = {"metric": "<O>+full-gradient/s", "value": world * 1e3 / g_per, "unit": "gradients/s",
                      "ms_per_eval": g_per, "forward_ms": ms_per_step, "cost_vs_forward": g_per / ms_per_step,
@@ -316,11 +320,7 @@ def main() -> None:
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_ms.append(dt * 1e3)
-    e2e_total = sum(e2e_ms)
-    if dist is not None:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(sum(e2e_ms), dist, dev)
     e2e = updates * world / (e2e_total / args.steps * 1e-3)
     h2d = int(gw.nbytes + ang.nbytes + keys.nbytes + coefs.nbytes)
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -31,6 +32,8 @@ thread_local std::string g_create_error;
 
 struct mpx_circuit {
     mpx::GateDesc *d_desc = nullptr;
+    uint64_t id = 0;         // unique per uploaded circuit (keys the engine's graph cache)
+    bool persistent = false; // uploaded by mpx_circuit_upload (worth a CUDA graph)
     uint64_t n = 0;
     std::vector<uint64_t> words; // host copy of the generators, for mpx_circuit_set_angles
     int W = 1;
@@ -91,10 +94,22 @@ struct mpx_engine {
     uint64_t n_sweep = 0;
     AdjointState adj;
     Tape fwd_tape{}; // tape fields the forward sweep fills (w_anti while recording a gradient)
+    // CUDA graphs of whole gate ranges of persistent circuits: captured after a propagation that did not
+    // grow the store, replayed while the store, its scratch and the truncation settings are unchanged.
+    struct GraphEntry {
+        uint64_t circuit_id, lo, hi, gen;
+        const uint32_t *w_anti;
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t store_gen = 0;
+    bool use_graphs = true;
     std::string err;
 };
 
 namespace {
+
+std::atomic<uint64_t> g_circuit_ids{1};
 
 #define MPX_CUDA(call)                                                                                              \
     do {                                                                                                            \
@@ -298,9 +313,16 @@ void free_store(mpx_engine *e) {
     e->sc.aux = nullptr;
 }
 
+void clear_graphs(mpx_engine *e) {
+    for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
+    e->graphs.clear();
+}
+
 // (Re)allocates the store for capacity `cap`, keeping the first n terms, and rebuilds the hash table.
 mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     mpx_engine *e = eng;
+    clear_graphs(e);
+    ++e->store_gen;
     const int W = e->W;
     if (cap >= 0xFFFFFFF0ULL) return fail(eng, MPX_ERR_CAPACITY, "term capacity exceeds the 32-bit term index");
     uint64_t *keys = nullptr;
@@ -372,6 +394,7 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
 mpx_status ensure_stats(mpx_engine *eng, uint64_t n) {
     mpx_engine *e = eng;
     if (n <= e->stats_cap) return MPX_OK;
+    clear_graphs(e); // the counters buffer is a kernel argument of every captured graph
     dev_free(e, e->d_stats);
     e->d_stats = nullptr;
     const uint64_t c = std::max<uint64_t>(n, 1024);
@@ -453,6 +476,7 @@ mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const doub
     MPX_CUDA(cudaStreamSynchronize(e->stream)); // h goes out of scope
     cd.n = n;
     cd.W = e->W;
+    cd.id = g_circuit_ids.fetch_add(1);
     cd.any_cos_zero = false;
     for (const GateDesc &g : h) cd.any_cos_zero = cd.any_cos_zero || g.cos_zero;
     cd.device = e->device;
@@ -471,6 +495,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     mpx_status s = ensure_stats(e, L);
     if (s != MPX_OK) return s;
     if (cd.any_cos_zero && !e->aux_on) {
+        clear_graphs(e);
         e->aux_on = true;
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->sc.aux), e->st.cap * sizeof(double)));
     }
@@ -487,6 +512,27 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     uint64_t chunk_id = 0;
     bool pending = false;
     uint64_t pending_slot = 0;
+    const uint64_t gen0 = e->store_gen;
+    const bool graphable = e->use_graphs && !e->profile && cd.persistent;
+    bool replayed = false;
+    if (graphable) {
+        for (const auto &g : e->graphs) {
+            if (g.circuit_id != cd.id || g.lo != lo || g.hi != hi || g.gen != gen0 || g.w_anti != e->fwd_tape.w_anti)
+                continue;
+            // One launch for the whole range; a gate that would overflow stalls the rest (no-ops), and the
+            // host resumes from it below exactly as after a chunk.
+            MPX_CUDA(cudaGraphLaunch(g.exec, e->stream));
+            e->launches += 2 * (hi - lo);
+            MPX_CUDA(cudaMemcpyAsync(&e->h_snap[0], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+            MPX_CUDA(cudaEventRecord(e->ev[0], e->stream));
+            step = hi;
+            pending = true;
+            pending_slot = 0;
+            chunk_id = 1;
+            replayed = true;
+            break;
+        }
+    }
     for (;;) {
         bool issued = false;
         if (step < hi) {
@@ -533,6 +579,29 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     e->last_gates = L;
+    if (graphable && !replayed && e->store_gen == gen0 && e->h_cnt->err == 0) {
+        // the range ran without growing the store: capture it for the next call
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            for (uint64_t st = lo; st < hi; ++st) gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
+            ok = cudaStreamEndCapture(e->stream, &graph) == cudaSuccess && graph != nullptr;
+        }
+        ok = ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        if (ok) {
+            if (e->graphs.size() >= 16) {
+                cudaGraphExecDestroy(e->graphs.front().exec);
+                e->graphs.erase(e->graphs.begin());
+            }
+            e->graphs.push_back({cd.id, lo, hi, gen0, e->fwd_tape.w_anti, exec});
+        }
+        else {
+            e->use_graphs = false; // capture unavailable here: keep issuing kernels directly
+        }
+        cudaGetLastError();
+    }
     if (e->profile) {
         e->t_sweep_ms = e->t_resolve_ms = e->t_columns_ms = 0.0;
         for (uint64_t st = lo; st < hi; ++st) {
@@ -901,6 +970,7 @@ mpx_status mpx_circuit_upload(mpx_engine *e, const uint64_t *gen_words, const do
     auto *c = new (std::nothrow) mpx_circuit();
     if (c == nullptr) return fail(eng, MPX_ERR_NOMEM, "host allocation failed");
     mpx_status s = upload_circuit(e, gen_words, angles, n_layers, *c);
+    c->persistent = true;
     if (s != MPX_OK) {
         mpx_circuit_destroy(c);
         return s;
@@ -1020,6 +1090,7 @@ mpx_status mpx_reset(mpx_engine *e) {
 
 mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    clear_graphs(e); // truncation settings are kernel arguments baked into captured graphs
     e->cfg.cutoff = cutoff;
     e->tr.cutoff = cutoff;
     return MPX_OK;
@@ -1027,6 +1098,7 @@ mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff) {
 
 mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    clear_graphs(e); // truncation settings are kernel arguments baked into captured graphs
     if (has_value && e->tr.has_upper && e->tr.upper < value)
         return fail(e, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
     e->cfg.has_lower_atol = has_value;
@@ -1038,6 +1110,7 @@ mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value) {
 
 mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    clear_graphs(e); // truncation settings are kernel arguments baked into captured graphs
     if (has_value && e->tr.has_lower && value < e->tr.lower)
         return fail(e, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
     e->cfg.has_upper_atol = has_value;
@@ -1131,6 +1204,7 @@ void mpx_destroy(mpx_engine *e) {
     }
     free_adjoint(e);
     cudaStreamSynchronize(e->stream);
+    clear_graphs(e);
     free_store(e);
     cudaFree(e->d_cnt);
     cudaFreeHost(e->h_cnt);

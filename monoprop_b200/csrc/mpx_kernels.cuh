@@ -430,11 +430,27 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     pos = (pos + 1) & st.tmask;
                 }
             }
-            if (ball != 0) {
-                // Bit-columns of the appended terms (InvertedIndex::append_rows, InvertedIndex.h:178-193).
-                // The warp's indices are consecutive, so they touch at most two column words: per column
-                // the lanes' bits are combined by a warp reduction and OR-ed into each word once. Column
-                // bits of terms not yet appended are zero, so OR is enough.
+            if (ball != 0 && __popc(ball) <= 4) {
+                // Bit-columns of the appended terms (InvertedIndex::append_rows, InvertedIndex.h:178-193);
+                // column bits of terms not yet appended are zero, so OR is enough. Few appends in the
+                // warp: each lane ORs its own bits.
+                if (miss) {
+                    int pop = 0;
+                    const uint32_t bit = 1u << (idx & 31);
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        pop += __popcll(p[w]);
+                        for (uint64_t x = p[w]; x != 0; x &= x - 1)
+                            atomicOr(st.cols + static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1) *
+                                                   st.cstride + (idx >> 5),
+                                     bit);
+                    }
+                    if (pop & 1) atomicOr(st.cols + static_cast<uint64_t>(64 * W) * st.cstride + (idx >> 5), bit);
+                }
+            }
+            else if (ball != 0) {
+                // Many appends: the warp's indices are consecutive, so they touch at most two column
+                // words; per column the lanes' bits are combined by a warp reduction and OR-ed once.
                 const uint64_t j0 = first >> 5;
                 const uint32_t mybit = miss ? (1u << (idx & 31)) : 0u;
                 const bool upper = miss && ((idx >> 5) != j0);

@@ -1,0 +1,62 @@
+"""Host-side logic that needs no GPU: the bench's max-over-ranks timing on two gloo ranks, the batch
+API's argument checks and the autotuner's sampling."""
+
+import ctypes as C
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from monoprop_b200 import _native
+from monoprop_b200 import workloads as W
+from monoprop_b200.batch import Autotuner, signature
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    out[rank] = bench.max_over_ranks(10.0 + rank, dist, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert out[0] == out[1] == 11.0
+
+
+def test_batch_run_rejects_null_buffers_without_touching_a_device():
+    lib = _native.load()
+    cfg = _native.Config(1, 1, 4, 0, 0.0, 0, 0.0, 8, 0, 0, 0, 0)
+    err = C.create_string_buffer(256)
+    rc = lib.mpx_batch_run(C.byref(cfg), None, 3, None, err, 256)
+    assert rc == 1 and b"NULL" in err.value
+
+
+def test_autotuner_sample_is_depth_stratified():
+    batch = W.batch_ising50(40, seed=4)
+    sample = Autotuner(cache_path="/nonexistent/x.json", sample=8).calibration_sample(batch)
+    depths = sorted(wl.n_layers for wl in batch)
+    got = sorted(wl.n_layers for wl in sample)
+    assert len(sample) == 8 and got[0] == depths[0] and got[-1] >= depths[len(depths) * 3 // 4]
+    assert signature(batch).startswith("pauli-W2-c8-support")
