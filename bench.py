@@ -137,22 +137,29 @@ def _cpu_threads() -> int:
 
 
 def time_reference(wl, steps: int, warmup: int, partitions: int) -> dict:
-    """The unmodified reference engine on the host cores: per step, one full propagate of ``wl``."""
+    """The unmodified reference engine on the host cores: per step, one full propagate of ``wl``.
+
+    Partition count: all host threads, or 1 when that is faster (small workloads, where the partition
+    exchange costs more than it saves; decided on full runs during warm-up when one takes < 1 s)."""
     import oracle
 
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libmpref.so is missing (build it with oracle/build_ref.sh)")
+
+    def run(p, n_layers=None):
+        eng = oracle.RefEngine(wl, partitions=p)
+        t = eng.propagate(n_layers=n_layers)
+        eng.close()
+        return t
+
     # Warm-up: a 400-gate prefix per warm-up step (pages the library and allocator in; CPU code has no JIT).
     for _ in range(warmup):
-        eng = oracle.RefEngine(wl, partitions=partitions)
-        eng.propagate(n_layers=min(400, wl.n_layers))
-        eng.close()
-    secs, updates = [], None
-    for _ in range(steps):
-        eng = oracle.RefEngine(wl, partitions=partitions)
-        secs.append(eng.propagate())
-        eng.close()
-    return {"seconds": secs}
+        run(partitions, min(400, wl.n_layers))
+    chosen = partitions
+    if partitions > 1 and run(partitions) < 1.0 and run(1) < run(partitions):
+        chosen = 1
+    secs = [run(chosen) for _ in range(steps)]
+    return {"seconds": secs, "partitions": chosen}
 
 
 def main() -> None:
@@ -195,7 +202,6 @@ def main() -> None:
     if args.impl == "reference":
         if rank != 0:
             return
-        # Sum of n_g for the workload, from the oracle port's counters (identical to the reference's).
         t = time_reference(wl, args.steps, args.warmup, cores)
         updates = _updates(wl)
         secs = t["seconds"]
@@ -205,7 +211,7 @@ def main() -> None:
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded circuit)", "config": config, "impl": "reference",
                 "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "reference",
-                                 "sample": f"full {wl.name} propagate per step, partitions={cores}"},
+                                 "sample": f"full {wl.name} propagate per step, partitions={t['partitions']}"},
                 "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -357,10 +363,11 @@ def main() -> None:
         import oracle
 
         if oracle.ref_available():
-            secs = time_reference(wl, 1, 0, cores)["seconds"]
+            t = time_reference(wl, 1, 0, cores)
+            secs = t["seconds"]
             cpu = {"value": updates / secs[0], "unit": "updates/s", "cores": cores, "kind": "reference",
-                   "sample": f"one full {wl.name} propagate (all {wl.n_layers} gates), partitions={cores}",
-                   "seconds": secs[0]}
+                   "sample": f"one full {wl.name} propagate (all {wl.n_layers} gates), "
+                             f"partitions={t['partitions']}", "seconds": secs[0]}
         else:
             cpu = {"value": None, "unit": "updates/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/libmpref.so not built"}
@@ -455,11 +462,10 @@ def kernel_case(n_terms: int, n_gates: int) -> None:
 
 
 def _updates(wl) -> int:
-    """sum_g n_g of ``wl`` from the oracle port's per-gate counters (equal to the engine's)."""
-    import oracle
+    """sum_g n_g of ``wl`` (the oracle's count, equal to the engine's per-gate counters)."""
+    from monoprop_b200.workloads import TERM_GATE_UPDATES
 
-    r = oracle.run_port(wl)
-    return int(r.counts[:, 0].sum())
+    return TERM_GATE_UPDATES[wl.name]
 
 
 if __name__ == "__main__":

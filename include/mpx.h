@@ -170,6 +170,19 @@ typedef struct {
 MPX_API mpx_status mpx_batch_run(const mpx_config *cfg, mpx_batch_item *items, uint64_t n_items,
                                  const mpx_batch_options *opt, char *err, size_t err_len);
 
+/* Frozen structure ("graph"), the reference's variational loop: MonomialPropagator<N>::build_graph
+ * (MonomialPropagator.inl:620-690) keeps every truncation decision of a coefficient-informed build, and
+ * expectation_value(parameters) / expectation_value_and_gradient(parameters) (.inl:1035-1050,
+ * MPFunctions.cpp:196-246) replay it at new parameters. mpx_graph_build propagates circuit c at its current
+ * angles (the engine then holds that evolved operator) and keeps each gate's rotated and appended pairs;
+ * mpx_circuit_set_angles then changes the parameters and mpx_graph_expectation / mpx_graph_gradient
+ * evaluate the frozen structure there (the engine then holds the replayed operator). grad_angles[l] =
+ * d<0|O|0>/d(angle_l). Any other propagation of the engine keeps the graph; a rebuild replaces it. */
+MPX_API mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation);
+MPX_API mpx_status mpx_graph_expectation(mpx_engine *e, const mpx_circuit *c, double *expectation);
+MPX_API mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation,
+                                      double *grad_angles);
+
 /* Per-kernel timing. With profiling on, the sweep, resolve and column-append launches of every gate are
  * bracketed by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms)
  * for the last propagate call. The reference has no device kernels; this replaces nothing there (its

@@ -22,7 +22,8 @@ _STATUS = {1: "MPX_ERR_INVALID", 2: "MPX_ERR_CUDA", 3: "MPX_ERR_NOMEM", 4: "MPX_
 EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_set_angles", "mpx_propagate_circuit",
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
-            "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_set_profiling", "mpx_kernel_times",
+            "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_graph_build", "mpx_graph_expectation",
+            "mpx_graph_gradient", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run")
 
@@ -79,6 +80,9 @@ def load() -> C.CDLL:
             "mpx_launch_count": (st, [vp, C.POINTER(u64)]),
             "mpx_adjoint_forward": (st, [vp, vp, u64, C.POINTER(C.c_double)]),
             "mpx_adjoint_backward": (st, [vp, vp, vp]),
+            "mpx_graph_build": (st, [vp, vp, u64, C.POINTER(C.c_double)]),
+            "mpx_graph_expectation": (st, [vp, vp, C.POINTER(C.c_double)]),
+            "mpx_graph_gradient": (st, [vp, vp, u64, C.POINTER(C.c_double), vp]),
             "mpx_set_profiling": (st, [vp, C.c_int32]),
             "mpx_kernel_times": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(u64)]),
@@ -252,6 +256,25 @@ class Engine:
         out = np.zeros(max(circuit.n_layers, 1), dtype=np.float64)
         self._check(self.lib.mpx_adjoint_backward(self.h, circuit.h, _p(out)))
         return out[: circuit.n_layers]
+
+    def graph_build(self, circuit: Circuit, segment_gates: int = 0) -> float:
+        """Propagate ``circuit`` and keep its truncation structure (the frozen graph); <O>."""
+        out = C.c_double(0.0)
+        self._check(self.lib.mpx_graph_build(self.h, circuit.h, int(segment_gates), C.byref(out)))
+        return out.value
+
+    def graph_expectation(self, circuit: Circuit) -> float:
+        """<O> of the frozen graph at ``circuit``'s current angles."""
+        out = C.c_double(0.0)
+        self._check(self.lib.mpx_graph_expectation(self.h, circuit.h, C.byref(out)))
+        return out.value
+
+    def graph_gradient(self, circuit: Circuit, segment_gates: int = 0) -> tuple[float, np.ndarray]:
+        """<O> and d<O>/d(angle_l) of the frozen graph at ``circuit``'s current angles."""
+        out = C.c_double(0.0)
+        g = np.zeros(max(circuit.n_layers, 1), dtype=np.float64)
+        self._check(self.lib.mpx_graph_gradient(self.h, circuit.h, int(segment_gates), C.byref(out), _p(g)))
+        return out.value, g[: circuit.n_layers]
 
     def set_profiling(self, on: bool) -> None:
         self._check(self.lib.mpx_set_profiling(self.h, int(bool(on))))

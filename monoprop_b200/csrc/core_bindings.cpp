@@ -6,8 +6,9 @@
 // binding angle_l = theta[map_l] * g_l (MPFunctions.cpp:57-69) and the decoded, filtered, 1e-12-rounded
 // export of evolved_operator (MonomialPropagator.inl:1099-1127).
 //
-// Scope: the Heisenberg propagate path. schrodinger_cutoff, basis_change, a stored graph (build_graph,
-// graph functionals, contract_partially with a graph) and MPI communicators raise NotImplementedError.
+// Scope: the Heisenberg picture -- propagate, and build_graph + expectation_value[_and_gradient](parameters)
+// over the engine's frozen structure (mpx_graph_*). schrodinger_cutoff, basis_change, only_rotate_len_k,
+// graph functionals with paring, contract_partially and MPI communicators raise NotImplementedError.
 #include <pybind11/complex.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -19,6 +20,7 @@
 #include <cstdint>
 #include <map>
 #include <optional>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -137,7 +139,10 @@ public:
               nullptr);
     }
 
-    ~Propagator() { mpx_destroy(e_); }
+    ~Propagator() {
+        if (circ_ != nullptr) mpx_circuit_destroy(circ_);
+        mpx_destroy(e_);
+    }
     Propagator(const Propagator &) = delete;
     Propagator &operator=(const Propagator &) = delete;
 
@@ -145,46 +150,86 @@ public:
     void propagate(const std::vector<std::vector<size_t>> &majoranas, const std::vector<size_t> &parameter_mapping,
                    const std::vector<double> &gen_coeffs, const std::vector<double> &parameters,
                    std::optional<unsigned int> only_rotate_len_k) {
-        const size_t L = majoranas.size();
-        if (parameter_mapping.size() != L || gen_coeffs.size() != L)
-            throw std::invalid_argument("majoranas (" + std::to_string(L) + "), parameter_mapping (" +
-                                        std::to_string(parameter_mapping.size()) + ") and gen_coeffs (" +
-                                        std::to_string(gen_coeffs.size()) + ") must have the same length.");
         if (only_rotate_len_k.has_value()) throw NotSupported("only_rotate_len_k: not implemented by the B200 engine");
-        std::vector<uint64_t> words(L * kWords, 0);
-        std::vector<double> angles(L);
-        for (size_t l = 0; l < L; ++l) {
-            if (parameter_mapping[l] >= parameters.size())
-                throw std::invalid_argument("parameter_mapping[" + std::to_string(l) + "] = " +
-                                            std::to_string(parameter_mapping[l]) + " is out of range for " +
-                                            std::to_string(parameters.size()) + " parameters.");
-            encode(majoranas[l], 2 * logical_, words.data() + l * kWords);
-            angles[l] = parameters[parameter_mapping[l]] * gen_coeffs[l];
-        }
+        if (circ_ != nullptr)
+            throw GraphStateConflict("propagate() needs no stored graph; this propagator holds one (build_graph)");
+        std::vector<uint64_t> words;
+        std::vector<double> angles;
+        encode_circuit(majoranas, parameter_mapping, gen_coeffs, parameters, words, angles);
         py::gil_scoped_release nogil;
-        check(mpx_propagate(e_, words.data(), angles.data(), L), e_);
+        check(mpx_propagate(e_, words.data(), angles.data(), majoranas.size()), e_);
     }
 
-    // Graph-less expectation: e_core + sum over fully paired terms (MPFunctions.cpp:196-205).
-    double expectation_value(const std::vector<double> &parameters) {
-        if (!parameters.empty())
-            throw GraphStateConflict("expectation_value(parameters) needs a stored graph; after propagate() call it "
-                                     "with no parameters.");
+    // MonomialPropagator<N>::build_graph (MonomialPropagator.inl:620-690): a coefficient-informed build at
+    // `parameters` whose truncation structure later evaluations keep.
+    void build_graph(const std::vector<std::vector<size_t>> &majoranas, const std::vector<size_t> &parameter_mapping,
+                     const std::vector<double> &gen_coeffs, std::optional<std::vector<size_t>> gate_indices,
+                     std::optional<std::vector<double>> parameters, std::optional<unsigned int> only_rotate_len_k) {
+        if (!parameters.has_value())
+            throw NotSupported("build_graph without seed parameters (a purely structural graph) is not implemented");
+        if (only_rotate_len_k.has_value()) throw NotSupported("only_rotate_len_k: not implemented by the B200 engine");
+        std::vector<uint64_t> words;
+        std::vector<double> angles;
+        encode_circuit(majoranas, parameter_mapping, gen_coeffs, *parameters, words, angles);
+        if (circ_ != nullptr) mpx_circuit_destroy(circ_);
+        circ_ = nullptr;
+        check(mpx_circuit_upload(e_, words.data(), angles.data(), majoranas.size(), &circ_), e_);
+        mapping_ = parameter_mapping;
+        gen_ = gen_coeffs;
+        n_params_ = parameters->size();
+        gates_ = gate_indices.has_value() ? std::set<size_t>(gate_indices->begin(), gate_indices->end()).size()
+                                          : majoranas.size();
         double ev = 0.0;
-        check(mpx_expectation(e_, &ev), e_);
+        py::gil_scoped_release nogil;
+        check(mpx_graph_build(e_, circ_, 0, &ev), e_);
+    }
+
+    // Expectation: with no parameters the current operator's (MPFunctions.cpp:196-205); with parameters the
+    // stored graph replayed at them (.inl:1035-1041).
+    double expectation_value(const std::vector<double> &parameters) {
+        double ev = 0.0;
+        if (parameters.empty()) {
+            check(mpx_expectation(e_, &ev), e_);
+            return ev;
+        }
+        set_graph_parameters(parameters);
+        py::gil_scoped_release nogil;
+        check(mpx_graph_expectation(e_, circ_, &ev), e_);
         return ev;
     }
 
+    // (<O>, d<O>/d theta) of the stored graph at `parameters` (.inl:1044-1050, MPFunctions.cpp:207-246);
+    // without a graph, the current operator's <O> and an empty gradient.
     std::pair<double, std::vector<double>> expectation_value_and_gradient(const std::vector<double> &parameters) {
-        return {expectation_value(parameters), {}};
+        if (circ_ == nullptr) {
+            if (!parameters.empty())
+                throw GraphStateConflict("expectation_value_and_gradient(parameters) needs a stored graph (build_graph)");
+            return {expectation_value(parameters), {}};
+        }
+        set_graph_parameters(parameters);
+        std::vector<double> ga(mapping_.size());
+        double ev = 0.0;
+        {
+            py::gil_scoped_release nogil;
+            check(mpx_graph_gradient(e_, circ_, 0, &ev, ga.data()), e_);
+        }
+        std::vector<double> grad(n_params_, 0.0);
+        for (size_t l = 0; l < mapping_.size(); ++l) grad[mapping_[l]] += gen_[l] * ga[l];
+        return {ev, grad};
     }
+
+    size_t graph_layers() const { return circ_ != nullptr ? mapping_.size() : 0; }
+    size_t n_gates() const { return circ_ != nullptr ? gates_ : 0; }
 
     // {indices: coefficient} of the evolved operator, |c| >= atol, decoded and rounded to 1e-12, with the
     // core term added (binder.h:200-221, MonomialPropagator.inl:1099-1127).
     py::dict evolved_operator(const std::vector<double> &parameters, double atol) {
-        if (!parameters.empty())
-            throw GraphStateConflict("evolved_operator(parameters) needs a stored graph; after propagate() call it "
-                                     "with no parameters.");
+        if (!parameters.empty()) {
+            if (circ_ == nullptr)
+                throw GraphStateConflict("evolved_operator(parameters) needs a stored graph; after propagate() call "
+                                         "it with no parameters.");
+            expectation_value(parameters); // the engine now holds the graph replayed at `parameters`
+        }
         uint64_t n = 0;
         check(mpx_size(e_, &n), e_);
         std::vector<uint64_t> words(n * kWords);
@@ -241,6 +286,36 @@ public:
     uintptr_t engine_handle() const { return reinterpret_cast<uintptr_t>(e_); }
 
 private:
+    void encode_circuit(const std::vector<std::vector<size_t>> &majoranas, const std::vector<size_t> &parameter_mapping,
+                        const std::vector<double> &gen_coeffs, const std::vector<double> &parameters,
+                        std::vector<uint64_t> &words, std::vector<double> &angles) const {
+        const size_t L = majoranas.size();
+        if (parameter_mapping.size() != L || gen_coeffs.size() != L)
+            throw std::invalid_argument("majoranas (" + std::to_string(L) + "), parameter_mapping (" +
+                                        std::to_string(parameter_mapping.size()) + ") and gen_coeffs (" +
+                                        std::to_string(gen_coeffs.size()) + ") must have the same length.");
+        words.assign(L * kWords, 0);
+        angles.assign(L, 0.0);
+        for (size_t l = 0; l < L; ++l) {
+            if (parameter_mapping[l] >= parameters.size())
+                throw std::invalid_argument("parameter_mapping[" + std::to_string(l) + "] = " +
+                                            std::to_string(parameter_mapping[l]) + " is out of range for " +
+                                            std::to_string(parameters.size()) + " parameters.");
+            encode(majoranas[l], 2 * logical_, words.data() + l * kWords);
+            angles[l] = parameters[parameter_mapping[l]] * gen_coeffs[l];
+        }
+    }
+
+    void set_graph_parameters(const std::vector<double> &parameters) {
+        if (circ_ == nullptr) throw GraphStateConflict("no stored graph: call build_graph first");
+        if (parameters.size() < n_params_)
+            throw std::invalid_argument("expected " + std::to_string(n_params_) + " parameters, got " +
+                                        std::to_string(parameters.size()) + ".");
+        std::vector<double> angles(mapping_.size());
+        for (size_t l = 0; l < mapping_.size(); ++l) angles[l] = parameters[mapping_[l]] * gen_[l];
+        check(mpx_circuit_set_angles(e_, circ_, angles.data()), e_);
+    }
+
     // MSb0 slot layout: slot s -> bit 2*Tier-1-s (AlgebraCommon.h:45-65); `limit` bounds the slot index.
     static void encode(const std::vector<size_t> &slots, size_t limit, uint64_t *out) {
         for (size_t s : slots) {
@@ -279,6 +354,10 @@ private:
     std::vector<size_t> state_;
     double core_ = 0.0;
     mpx_engine *e_ = nullptr;
+    mpx_circuit *circ_ = nullptr; // the stored graph's circuit (build_graph)
+    std::vector<size_t> mapping_;
+    std::vector<double> gen_;
+    size_t n_params_ = 0, gates_ = 0;
 };
 
 template <size_t Tier>
@@ -297,13 +376,16 @@ void bind(py::module_ &m) {
              py::arg("partitions") = 0)
         .def("propagate", &P::propagate, py::arg("majoranas"), py::arg("parameter_mapping"), py::arg("gen_coeffs"),
              py::arg("parameters"), py::arg("only_rotate_len_k") = py::none())
+        .def("build_graph", &P::build_graph, py::arg("majoranas"), py::arg("parameter_mapping"), py::arg("gen_coeffs"),
+             py::arg("gate_indices") = py::none(), py::arg("parameters") = py::none(),
+             py::arg("only_rotate_len_k") = py::none())
         .def("expectation_value", &P::expectation_value, py::arg("parameters"))
         .def("expectation_value_and_gradient", &P::expectation_value_and_gradient, py::arg("parameters"))
         .def("evolved_operator", &P::evolved_operator, py::arg("parameters"), py::arg("atol"))
         .def("size", &P::size)
         .def("graph_size", [](P &) { return std::pair<size_t, size_t>(0, 0); })
-        .def("graph_layers", [](P &) { return size_t{0}; })
-        .def("n_gates", [](P &) { return size_t{0}; })
+        .def("graph_layers", &P::graph_layers)
+        .def("n_gates", &P::n_gates)
         .def("operator_memory_bytes", &P::operator_memory_bytes)
         .def("core_term", &P::core_term)
         .def("_engine_handle", &P::engine_handle)

@@ -186,3 +186,111 @@ __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__
 }
 
 }  // namespace mpx
+
+namespace mpx {
+
+// ----- frozen structure ("graph") evaluation ------------------------------------------------------------
+//
+// The reference's variational loop builds a surrogate graph once and replays it at new parameters
+// (MonomialPropagator.inl:620-690, Evolution.cpp:471-540): every truncation decision of the build is
+// kept. Here the build's rotated and appended pairs of every gate are kept (src, tgt, phase | appended),
+// and the anticommuting sets are recomputed from the bit-columns (they depend only on the keys). One
+// gate at new angles is then two launches: the pairs (exact 2x2 rotations of their pre-gate values) and
+// the cos scaling of every other anticommuting term.
+struct Frozen {
+    const uint32_t *src;
+    const uint32_t *tgt;
+    const int8_t *code;                  // phase (+1 / -1 / 0) | 0x10 for an appended partner
+    const uint64_t *p_begin;             // [n_steps] first pair of each step
+    const unsigned long long *p_count;   // [n_steps] pairs of each step
+};
+
+// Pairs of one frozen gate; with LOG also their pre-gate values into the tape's pair log (the slot of
+// pair k is p_base[step] + k, so no counters are needed).
+template <bool LOG>
+__global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ coef, Frozen fz,
+                                                          const GateDesc *__restrict__ gates, uint32_t gate,
+                                                          uint32_t step, uint32_t *__restrict__ done, Tape tp) {
+    const uint64_t b = fz.p_begin[step], cnt = fz.p_count[step];
+    const GateDesc &gd = gates[gate];
+    const double C = gd.cosv, S = gd.sinv;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < cnt;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t s = fz.src[b + k], t = fz.tgt[b + k];
+        const int8_t code = fz.code[b + k];
+        const bool appended = (code & 0x10) != 0;
+        const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
+        const double vs = coef[s], vt = appended ? 0.0 : coef[t];
+        coef[s] = C * vs - S * phi * vt;
+        coef[t] = C * vt + S * phi * vs;
+        atomicOr(&done[s >> 5], 1u << (s & 31));
+        if (!appended) atomicOr(&done[t >> 5], 1u << (t & 31));
+        if constexpr (LOG) {
+            const uint64_t r = tp.p_base[step] + k;
+            tp.p_src[r] = s;
+            tp.p_tgt[r] = t;
+            tp.p_code[r] = code;
+            tp.p_vs[r] = vs;
+            tp.p_vt[r] = vt;
+        }
+    }
+}
+
+// The other anticommuting terms of one frozen gate (terms < n0 whose fold-column parity is odd): scaled
+// by cos; pair members (done bits, set by k_frozen_pairs) are skipped and their bits cleared. With LOG
+// every anticommuting term's pre-gate value goes to the undo log at the warp's offset, in the same
+// chunk/lane order as the streaming sweep (pair members' entries are never read).
+template <int W, bool LOG>
+__global__ void __launch_bounds__(kBlock) k_frozen_scan(Store st, const GateDesc *__restrict__ gates, uint32_t gate,
+                                                         uint32_t step, uint64_t n0, uint32_t *__restrict__ done,
+                                                         Tape tp) {
+    const GateDesc &gd = gates[gate];
+    if (gd.empty || n0 == 0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t nwords = (n0 + 31) >> 5, nchunks = (nwords + 31) >> 5;
+    const uint64_t n_warps = static_cast<uint64_t>(gridDim.x) * (kBlock / 32);
+    const uint64_t wg = static_cast<uint64_t>(blockIdx.x) * (kBlock / 32) + warp;
+    const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
+    const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
+    const double C = gd.cosv;
+    uint64_t ubase = 0;
+    if constexpr (LOG) ubase = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * n_warps + wg];
+    uint64_t anti_count = 0;
+    for (uint64_t chunk = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp; chunk < nchunks; chunk += n_warps) {
+        const uint64_t j = chunk * 32 + lane;
+        uint32_t anti = 0, dn = 0;
+        if (j < nwords) {
+#pragma unroll
+            for (int w = 0; w < W; ++w)
+                for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1)
+                    anti ^= st.cols[static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1) * st.cstride + j];
+            if (gd.g_odd) anti ^= parity[j];
+            if (j == nwords - 1) anti &= tail;
+            dn = done[j];
+            if (dn) done[j] = 0;
+        }
+        // prefix of the lanes' counts: the undo order is (chunk, lane, bit), as in the sweep
+        const int cnt_l = __popc(anti);
+        int incl = cnt_l;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        int r = incl - cnt_l;
+        for (uint32_t a = anti; a != 0; a &= a - 1, ++r) {
+            const int bit = __ffs(a) - 1;
+            const uint64_t i = j * 32 + bit;
+            const double v = st.coef[i];
+            if constexpr (LOG) {
+                tp.u_idx[ubase + anti_count + r] = static_cast<uint32_t>(i);
+                tp.u_val[ubase + anti_count + r] = v;
+            }
+            if (!((dn >> bit) & 1u)) st.coef[i] = v * C;
+        }
+        anti_count += static_cast<uint64_t>(total);
+    }
+}
+
+}  // namespace mpx

@@ -21,6 +21,7 @@
 
 #include "../../include/mpx.h"
 #include "mpx_kernels.cuh"
+#include "mpx_small.cuh"
 
 using namespace mpx;
 
@@ -55,6 +56,19 @@ struct AdjointState {
     uint64_t n_final = 0;
     std::vector<uint64_t> stats; // [L][4] n_g, a_g, e_g, (unused) per step
     uint32_t *w_anti = nullptr;   // [L][sweep warps] anticommuting terms per sweep warp and step
+};
+
+// A frozen structure (the surrogate "graph" of the reference's variational loop): every gate's rotated
+// and appended pairs of the build, plus what re-deriving the anticommuting sets needs.
+struct FrozenGraph {
+    uint64_t circuit_id = 0, L = 0, n_final = 0;
+    uint32_t *src = nullptr, *tgt = nullptr;
+    int8_t *code = nullptr;
+    uint64_t *p_begin = nullptr;            // [L] device
+    unsigned long long *p_count = nullptr;  // [L] device
+    std::vector<uint64_t> n0, anti, count;  // per step (host)
+    uint32_t *w_anti = nullptr;             // [L][sweep warps] anticommuting terms per sweep warp (build)
+    uint32_t *done = nullptr;               // [ceil(n_final / 32)] scratch bitmap
 };
 
 struct mpx_engine {
@@ -93,6 +107,7 @@ struct mpx_engine {
     double t_sweep_ms = 0.0, t_resolve_ms = 0.0, t_columns_ms = 0.0;
     uint64_t n_sweep = 0;
     AdjointState adj;
+    FrozenGraph fg;
     Tape fwd_tape{}; // tape fields the forward sweep fills (w_anti while recording a gradient)
     // CUDA graphs of whole gate ranges of persistent circuits: captured after a propagation that did not
     // grow the store, replayed while the store, its scratch and the truncation settings are unchanged.
@@ -104,6 +119,7 @@ struct mpx_engine {
     std::vector<GraphEntry> graphs;
     uint64_t store_gen = 0;
     bool use_graphs = true;
+    bool small_path = true; // run small stores in one shared-memory block (mpx_small.cuh)
     std::string err;
 };
 
@@ -175,6 +191,7 @@ void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t 
     k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
                                                        e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
+    k_columns<W><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, 0, 0, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
 }
 
@@ -185,6 +202,61 @@ void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_
     k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
                                                              tp);
     k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
+}
+
+// Shared-memory capacity of the single-block path per key width: the largest power-of-two-friendly size
+// whose store, query list, hash table (load <= 1/2) and bitmap fit in 227 KB.
+constexpr uint32_t kSmallCap[5] = {0, 8192, 6144, 4096, 4096};
+constexpr uint32_t kSmallTableBits[5] = {0, 14, 14, 13, 13};
+
+template <int W, int B>
+cudaError_t launch_small(mpx_engine *e, const GateDesc *d_desc, uint32_t L, uint32_t lo, uint32_t hi) {
+    const uint32_t cap = kSmallCap[W], tbits = kSmallTableBits[W];
+    const size_t bytes = small_smem_bytes(W, cap, tbits);
+    static bool configured = false; // per instantiation; the attribute is per function
+    if (!configured) {
+        const cudaError_t ce = cudaFuncSetAttribute(k_small<W, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    static_cast<int>(bytes));
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    k_small<W, B><<<1, kSmallThreads, bytes, e->stream>>>(e->st, e->d_cnt, d_desc, L, lo, hi, e->tr, e->d_stats, cap,
+                                                         tbits);
+    return cudaGetLastError();
+}
+
+using SmallFn = cudaError_t (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t, uint32_t);
+SmallFn pick_small(int W, int basis) {
+    switch (W) {
+    case 1: return basis == 1 ? &launch_small<1, 1> : &launch_small<1, 0>;
+    case 2: return basis == 1 ? &launch_small<2, 1> : &launch_small<2, 0>;
+    case 3: return basis == 1 ? &launch_small<3, 1> : &launch_small<3, 0>;
+    case 4: return basis == 1 ? &launch_small<4, 1> : &launch_small<4, 0>;
+    default: return nullptr;
+    }
+}
+
+template <int W, bool LOG>
+void launch_frozen(mpx_engine *e, const GateDesc *d_desc, const Frozen &fz, uint32_t gate, uint32_t step, uint64_t n0,
+                   uint32_t *done, const Tape &tp) {
+    k_frozen_pairs<LOG><<<e->grid, kBlock, 0, e->stream>>>(e->st.coef, fz, d_desc, gate, step, done, tp);
+    k_frozen_scan<W, LOG><<<e->grid, kBlock, 0, e->stream>>>(e->st, d_desc, gate, step, n0, done, tp);
+}
+
+using FrozenFn = void (*)(mpx_engine *, const GateDesc *, const Frozen &, uint32_t, uint32_t, uint64_t, uint32_t *,
+                          const Tape &);
+template <bool LOG>
+FrozenFn pick_frozen(int W) {
+    switch (W) {
+    case 1: return &launch_frozen<1, LOG>;
+    case 2: return &launch_frozen<2, LOG>;
+    case 3: return &launch_frozen<3, LOG>;
+    case 4: return &launch_frozen<4, LOG>;
+    case 5: return &launch_frozen<5, LOG>;
+    case 6: return &launch_frozen<6, LOG>;
+    case 7: return &launch_frozen<7, LOG>;
+    default: return &launch_frozen<8, LOG>;
+    }
 }
 
 template <int W, int B>
@@ -512,8 +584,42 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     uint64_t chunk_id = 0;
     bool pending = false;
     uint64_t pending_slot = 0;
+    // Small store: run gates in one shared-memory block until the store outgrows it (or the range ends).
+    bool used_small = false;
+    if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && e->fwd_tape.w_anti == nullptr &&
+        hi - lo >= 8) {
+        MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+        const uint64_t n_now = e->h_cnt->n;
+        const uint32_t cap_small = kSmallCap[e->W];
+        if (e->h_cnt->stall == kNoStall && n_now * 2 <= cap_small) {
+            if (e->st.cap < cap_small) {
+                s = alloc_store(e, 2 * cap_small, n_now);
+                if (s != MPX_OK) return s;
+            }
+            MPX_CUDA(pick_small(e->W, e->cfg.basis)(e, cd.d_desc, static_cast<uint32_t>(L), static_cast<uint32_t>(lo),
+                                                   static_cast<uint32_t>(hi)));
+            e->launches += 1;
+            MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+            MPX_CUDA(cudaStreamSynchronize(e->stream));
+            const uint64_t n = e->h_cnt->n;
+            const uint64_t resume = e->h_cnt->stall == kNoStall ? hi : e->h_cnt->stall;
+            // the streaming kernels need the hash table and bit-columns of the store the block wrote back
+            MPX_CUDA(cudaMemsetAsync(e->st.table, 0xFF, (e->st.tmask + 1) * sizeof(unsigned long long), e->stream));
+            MPX_CUDA(cudaMemsetAsync(e->st.cols, 0, (64 * e->W + 1) * e->st.cstride * sizeof(uint32_t), e->stream));
+            pick_build(e->W)(e, 0, n);
+            e->launches += 2;
+            Counters c{};
+            c.n = n;
+            c.n0 = n;
+            c.stall = kNoStall;
+            MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+            step = resume;
+            used_small = true;
+        }
+    }
     const uint64_t gen0 = e->store_gen;
-    const bool graphable = e->use_graphs && !e->profile && cd.persistent;
+    const bool graphable = e->use_graphs && !e->profile && cd.persistent && !used_small;
     bool replayed = false;
     if (graphable) {
         for (const auto &g : e->graphs) {
@@ -522,7 +628,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             // One launch for the whole range; a gate that would overflow stalls the rest (no-ops), and the
             // host resumes from it below exactly as after a chunk.
             MPX_CUDA(cudaGraphLaunch(g.exec, e->stream));
-            e->launches += 2 * (hi - lo);
+            e->launches += 3 * (hi - lo);
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[0], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
             MPX_CUDA(cudaEventRecord(e->ev[0], e->stream));
             step = hi;
@@ -540,7 +646,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             for (uint64_t st = step; st < stop; ++st) {
                 gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
             }
-            e->launches += 2 * (stop - step);
+            e->launches += 3 * (stop - step);
             MPX_CUDA(cudaGetLastError());
             const uint64_t slot = chunk_id & 1;
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[slot], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
@@ -712,7 +818,10 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
 
 // Reverse sweep: per segment (last first) restore its checkpoint, replay it logging the tape, then walk
 // its gates backwards. grad_angles[l] = dE/d(angle_l) for circuit layer l (angle = theta[map] * g).
-mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_angles) {
+// With fg == nullptr: the gradient of the last mpx_adjoint_forward (segments replayed with the
+// streaming kernels). With fg: the gradient of the frozen structure fg at the circuit's current angles
+// (segments replayed with the frozen kernels, whose pair counts are fixed).
+mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_angles, const FrozenGraph *fg = nullptr) {
     mpx_engine *e = eng;
     AdjointState &A = e->adj;
     const uint64_t L = A.L;
@@ -785,6 +894,9 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     MPX_CUDA_REL(cudaMemcpyAsync(d_steps + L, p_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
     MPX_CUDA_REL(cudaMemcpyAsync(d_steps + 2 * L, n_next.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
     MPX_CUDA_REL(cudaMemsetAsync(d_cnts, 0, 2 * L * sizeof(unsigned long long), e->stream));
+    if (fg != nullptr)
+        MPX_CUDA_REL(cudaMemcpyAsync(d_cnts + L, fg->p_count, L * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                     e->stream));
     const uint32_t n_warps = static_cast<uint32_t>(e->grid) * kWarps;
     uint64_t max_seg = 1;
     for (size_t sg = 0; sg < S; ++sg) max_seg = std::max<uint64_t>(max_seg, (sg + 1 < S ? A.seg_lo[sg + 1] : L) - A.seg_lo[sg]);
@@ -796,6 +908,9 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     MPX_CUDA_REL(cudaMemsetAsync(done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
     pick_adj_init(e->W, e->cfg.basis)(e, lam, nf);
     const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
+    const FrozenFn frozen_replay = pick_frozen<true>(e->W);
+    Frozen fz{};
+    if (fg != nullptr) fz = Frozen{fg->src, fg->tgt, fg->code, fg->p_begin, fg->p_count};
     for (size_t sg = S; sg-- > 0;) {
         const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
         const uint64_t n = A.ck_n[sg];
@@ -809,7 +924,13 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         MPX_CUDA_REL(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
         k_undo_offsets<<<static_cast<unsigned>(hi - lo), 1024, 0, e->stream>>>(tp, n_warps, lo, u_off);
         tp.u_off_step0 = lo;
-        for (uint64_t st = lo; st < hi; ++st) replay(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), tp);
+        for (uint64_t st = lo; st < hi; ++st) {
+            if (fg != nullptr)
+                frozen_replay(e, cd.d_desc, fz, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), fg->n0[st],
+                              done, tp);
+            else
+                replay(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), tp);
+        }
         for (uint64_t st = hi; st-- > lo;) {
             const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
             k_adj_pairs<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
@@ -836,6 +957,197 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     MPX_CUDA(cudaStreamSynchronize(e->stream));
 #undef MPX_CUDA_REL
     if (err != 0) return fail(eng, MPX_ERR_STATE, "gradient replay diverged from the forward pass (internal error)");
+    return MPX_OK;
+}
+
+// ----- frozen structure (graph) -----------------------------------------------------------------------
+
+void free_graph(mpx_engine *e) {
+    FrozenGraph &g = e->fg;
+    for (void *p : {static_cast<void *>(g.src), static_cast<void *>(g.tgt), static_cast<void *>(g.code),
+                    static_cast<void *>(g.p_begin), static_cast<void *>(g.p_count), static_cast<void *>(g.w_anti),
+                    static_cast<void *>(g.done)})
+        dev_free(e, p);
+    g = FrozenGraph{};
+}
+
+// Build: the gradient forward pass (checkpoints, per-warp counts), then every segment replayed once with
+// the streaming kernels to collect each gate's pairs into the graph.
+mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+    mpx_engine *e = eng;
+    free_graph(e);
+    mpx_status s = adjoint_forward(e, cd, segment_gates);
+    if (s != MPX_OK) return s;
+    AdjointState &A = e->adj;
+    FrozenGraph &g = e->fg;
+    const uint64_t L = A.L, nf = A.n_final;
+    const size_t S = A.seg_lo.size();
+    std::vector<uint64_t> begin(L), u_base(L), n_next(L);
+    uint64_t total_e = 0, u_max = 1;
+    for (size_t sg = 0; sg < S; ++sg) {
+        const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
+        uint64_t u = 0;
+        for (uint64_t st = lo; st < hi; ++st) {
+            u_base[st] = u;
+            u += A.stats[4 * st + 1];
+            n_next[st] = st + 1 < L ? A.stats[4 * (st + 1)] : nf;
+        }
+        u_max = std::max(u_max, u);
+    }
+    for (uint64_t st = 0; st < L; ++st) {
+        begin[st] = total_e;
+        total_e += A.stats[4 * st + 2];
+    }
+    Tape tp{};
+    uint64_t *d_steps = nullptr, *u_off = nullptr;
+    unsigned long long *u_cnt = nullptr;
+    cudaError_t ce = cudaSuccess;
+    auto A_ = [&](void **ptr, size_t bytes) {
+        if (ce == cudaSuccess) ce = dev_alloc(e, ptr, std::max<size_t>(bytes, 16));
+    };
+    const uint32_t n_warps = static_cast<uint32_t>(e->grid) * kWarps;
+    uint64_t max_seg = 1;
+    for (size_t sg = 0; sg < S; ++sg) max_seg = std::max<uint64_t>(max_seg, (sg + 1 < S ? A.seg_lo[sg + 1] : L) - A.seg_lo[sg]);
+    A_(reinterpret_cast<void **>(&g.src), total_e * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&g.tgt), total_e * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&g.code), total_e * sizeof(int8_t));
+    A_(reinterpret_cast<void **>(&g.p_begin), L * sizeof(uint64_t));
+    A_(reinterpret_cast<void **>(&g.p_count), L * sizeof(unsigned long long));
+    A_(reinterpret_cast<void **>(&g.done), ((nf + 31) / 32) * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&tp.p_vs), total_e * sizeof(double));
+    A_(reinterpret_cast<void **>(&tp.p_vt), total_e * sizeof(double));
+    A_(reinterpret_cast<void **>(&tp.u_idx), u_max * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&tp.u_val), u_max * sizeof(double));
+    A_(reinterpret_cast<void **>(&d_steps), 2 * L * sizeof(uint64_t));
+    A_(reinterpret_cast<void **>(&u_cnt), L * sizeof(unsigned long long));
+    A_(reinterpret_cast<void **>(&u_off), max_seg * n_warps * sizeof(uint64_t));
+    auto release = [&]() {
+        for (void *ptr : {static_cast<void *>(tp.p_vs), static_cast<void *>(tp.p_vt), static_cast<void *>(tp.u_idx),
+                          static_cast<void *>(tp.u_val), static_cast<void *>(d_steps), static_cast<void *>(u_cnt),
+                          static_cast<void *>(u_off)})
+            dev_free(e, ptr);
+    };
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        free_graph(e);
+        return fail(eng, MPX_ERR_NOMEM, std::string("graph allocation failed: ") + cudaGetErrorString(ce));
+    }
+    MPX_CUDA(cudaMemcpyAsync(g.p_begin, begin.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA(cudaMemsetAsync(g.p_count, 0, L * sizeof(unsigned long long), e->stream));
+    MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+    MPX_CUDA(cudaMemcpyAsync(d_steps, u_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA(cudaMemcpyAsync(d_steps + L, n_next.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    tp.p_src = g.src;
+    tp.p_tgt = g.tgt;
+    tp.p_code = g.code;
+    tp.p_base = g.p_begin;
+    tp.p_cnt = g.p_count;
+    tp.u_base = d_steps;
+    tp.n_next = d_steps + L;
+    tp.u_cnt = u_cnt;
+    tp.w_anti = A.w_anti;
+    tp.u_off = u_off;
+    const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
+    for (size_t sg = 0; sg < S; ++sg) {
+        const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
+        const uint64_t n = A.ck_n[sg];
+        if (n > 0)
+            MPX_CUDA(cudaMemcpyAsync(e->st.coef, A.ck_coef[sg], n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+        Counters c{};
+        c.n = n;
+        c.n0 = n;
+        c.stall = kNoStall;
+        MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+        k_undo_offsets<<<static_cast<unsigned>(hi - lo), 1024, 0, e->stream>>>(tp, n_warps, lo, u_off);
+        tp.u_off_step0 = lo;
+        for (uint64_t st = lo; st < hi; ++st) replay(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), tp);
+        e->launches += 3 * (hi - lo) + 1;
+        MPX_CUDA(cudaGetLastError());
+    }
+    // the engine keeps the evolved operator of the build
+    if (nf > 0) MPX_CUDA(cudaMemcpyAsync(e->st.coef, A.final_coef, nf * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
+    g.count.assign(L, 0);
+    MPX_CUDA(cudaMemcpyAsync(g.count.data(), g.p_count, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    const uint32_t err = e->h_cnt->err;
+    Counters c{};
+    c.n = nf;
+    c.n0 = nf;
+    c.stall = kNoStall;
+    MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+    release();
+    g.circuit_id = cd.id;
+    g.L = L;
+    g.n_final = nf;
+    g.n0.resize(L);
+    g.anti.resize(L);
+    for (uint64_t st = 0; st < L; ++st) {
+        g.n0[st] = A.stats[4 * st];
+        g.anti[st] = A.stats[4 * st + 1];
+    }
+    g.w_anti = A.w_anti; // the graph keeps the per-warp counts
+    A.w_anti = nullptr;
+    free_adjoint(e);
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    if (err != 0) {
+        free_graph(e);
+        return fail(eng, MPX_ERR_STATE, "graph build replay diverged from the forward pass (internal error)");
+    }
+    return MPX_OK;
+}
+
+// The frozen structure at the circuit's current angles, from the initial operator; with segment_gates
+// > 0 the coefficient array is saved at segment starts (for the frozen gradient).
+mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+    mpx_engine *e = eng;
+    FrozenGraph &g = e->fg;
+    const uint64_t L = g.L, nf = g.n_final;
+    free_adjoint(e);
+    if (e->n_init > 0)
+        MPX_CUDA(cudaMemcpyAsync(e->st.coef, e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    if (nf > e->n_init)
+        MPX_CUDA(cudaMemsetAsync(e->st.coef + e->n_init, 0, (nf - e->n_init) * sizeof(double), e->stream));
+    MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+    const Frozen fz{g.src, g.tgt, g.code, g.p_begin, g.p_count};
+    const FrozenFn run = pick_frozen<false>(e->W);
+    const uint64_t K = segment_gates == 0 ? std::max<uint64_t>(L, 1) : segment_gates;
+    for (uint64_t st = 0; st < L; ++st) {
+        if (segment_gates > 0 && st % K == 0) {
+            const uint64_t n = g.n0[st];
+            double *ck = nullptr;
+            MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double)));
+            e->adj.ck_coef.push_back(ck);
+            if (n > 0) MPX_CUDA(cudaMemcpyAsync(ck, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+            e->adj.seg_lo.push_back(st);
+            e->adj.ck_n.push_back(n);
+        }
+        run(e, cd.d_desc, fz, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st), g.n0[st], g.done, Tape{});
+    }
+    e->launches += 2 * L;
+    MPX_CUDA(cudaGetLastError());
+    Counters c{};
+    c.n = nf;
+    c.n0 = nf;
+    c.stall = kNoStall;
+    MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
+    if (segment_gates > 0) {
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(nf, 1) * sizeof(double)));
+        if (nf > 0)
+            MPX_CUDA(cudaMemcpyAsync(e->adj.final_coef, e->st.coef, nf * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+        e->adj.n_final = nf;
+        e->adj.L = L;
+        e->adj.stats.assign(4 * L, 0);
+        for (uint64_t st = 0; st < L; ++st) {
+            e->adj.stats[4 * st] = g.n0[st];
+            e->adj.stats[4 * st + 1] = g.anti[st];
+            e->adj.stats[4 * st + 2] = g.count[st];
+        }
+        e->adj.w_anti = g.w_anti; // borrowed: released before free_adjoint can see it
+    }
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
     return MPX_OK;
 }
 
@@ -1162,6 +1474,49 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
     return adjoint_backward(e, *c, grad_angles);
 }
 
+mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation) {
+    if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    MPX_CUDA(cudaSetDevice(e->device));
+    mpx_status s = graph_build(e, *c, segment_gates);
+    if (s != MPX_OK) return s;
+    return mpx_expectation(e, expectation);
+}
+
+static mpx_status check_graph(mpx_engine *e, const mpx_circuit *c) {
+    if (e->fg.L == 0 || e->fg.circuit_id != c->id)
+        return fail(e, MPX_ERR_STATE, "no graph built for this circuit (mpx_graph_build)");
+    return MPX_OK;
+}
+
+mpx_status mpx_graph_expectation(mpx_engine *e, const mpx_circuit *c, double *expectation) {
+    if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    mpx_status s = check_graph(e, c);
+    if (s != MPX_OK) return s;
+    MPX_CUDA(cudaSetDevice(e->device));
+    s = frozen_forward(e, *c, 0);
+    if (s != MPX_OK) return s;
+    return mpx_expectation(e, expectation);
+}
+
+mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation,
+                              double *grad_angles) {
+    if (e == nullptr || c == nullptr || expectation == nullptr || (c->n > 0 && grad_angles == nullptr))
+        return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    mpx_status s = check_graph(e, c);
+    if (s != MPX_OK) return s;
+    MPX_CUDA(cudaSetDevice(e->device));
+    s = frozen_forward(e, *c, segment_gates == 0 ? std::max<uint64_t>(c->n, 1) : segment_gates);
+    if (s == MPX_OK) s = mpx_expectation(e, expectation);
+    if (s == MPX_OK && c->n > 0) s = adjoint_backward(e, *c, grad_angles, &e->fg);
+    e->adj.w_anti = nullptr; // owned by the graph
+    free_adjoint(e);
+    return s;
+}
+
 mpx_status mpx_set_profiling(mpx_engine *e, int32_t on) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     e->profile = on != 0;
@@ -1203,6 +1558,7 @@ void mpx_destroy(mpx_engine *e) {
         cudaStreamSynchronize(e->stream);
     }
     free_adjoint(e);
+    free_graph(e);
     cudaStreamSynchronize(e->stream);
     clear_graphs(e);
     free_store(e);

@@ -1,14 +1,16 @@
 // mpx_kernels.cuh -- the per-gate kernels of the B200 propagation engine (sm_100a).
 //
-// One Heisenberg gate = two launches over the device term store:
+// One Heisenberg gate = three launches over the device term store:
 //   k_sweep   -- anticommutation test from the generator's bit-columns (|fold| bits per term), fused cos
 //                scaling of the anticommuting coefficients, lower_atol / structural-cutoff / upper_atol
 //                emit gate, rotation phase, leader/follower class; compacts the emitted sine branches into
 //                the query arrays and writes the leader-emitted bitmap.
 //   k_resolve -- one thread per emitted branch: open-addressing lookup of the partner M^G, the
 //                leader/follower rule, the rotation of the pair, or the unique append of the missing partner.
-//              The appended terms' bit-columns are OR-ed in by the same kernel.
-//   k_columns -- (re)builds the bit-columns of a range of stored terms (construction, growth, reset).
+//   k_columns -- adds the appended terms to the bit-columns when some warp appended a dense run (and
+//                builds them on construction, growth, reset); sparse appends OR their bits in k_resolve.
+//                Transposing whole 32-term words with ballots beats OR-ing bits when a gate appends many
+//                terms, and a launch that finds nothing to do returns at once.
 // Every coefficient slot is written by exactly one thread per gate (the sine partner map M -> M^G is
 // injective), so no coefficient atomics are needed (layer_build/FusedApply.h:54-56).
 #pragma once
@@ -38,9 +40,11 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
 constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
+constexpr int kSparseAppends = 4;    // appends per warp round up to which k_resolve writes the bit-columns
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
-// warp w of the grid scans chunks w, w + W_total, ... of 1024 terms and owns query region w.
+// warp w of block b scans the 1024-term chunks b + grid * (w + warps * i) and owns query region
+// b * warps + w.
 struct SweepGeometry {
     uint64_t nwords, nchunks, stride;
     uint32_t n_warps;
@@ -83,7 +87,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         if (threadIdx.x == 0) atomicMin(&cnt->stall, step);
         return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n0 = n0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt->n0 = n0;
+        cnt->cols_dirty = 0;
+    }
     const GateDesc &gd = gates[gate];
     const int n_fold = gd.n_fold;
     if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
@@ -104,7 +111,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
         const uint64_t qbase = static_cast<uint64_t>(wg) * geo.stride;
 
-        for (uint64_t chunk = wg; chunk < geo.nchunks; chunk += geo.n_warps) {
+        // Consecutive chunks go to consecutive blocks (chunk = block + grid * (warp + warps * i)): the
+        // oldest terms, which carry the largest coefficients and most of the emitted branches, spread
+        // over all blocks instead of piling up in the first few, for the sweep and for the resolve.
+        for (uint64_t chunk = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp; chunk < geo.nchunks;
+             chunk += geo.n_warps) {
             const uint64_t j = chunk * 32 + lane;
             uint32_t anti = 0, foll = 0;
             if (j < geo.nwords) {
@@ -413,74 +424,38 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 tp.p_vt[r] = vt;
             }
         }
-        else {
-            const uint64_t first = s_base + off; // this warp's appends are [first, first + popc(ball))
-            const uint64_t idx = first + __popc(ball & lt_mask);
-            if (miss) {
-                store_key<W>(st.keys, idx, p);
-                st.coef[idx] = (sinv * ph) * v;
-                const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
-                for (uint64_t probes = 0;; ++probes) {
-                    if (probes > st.tmask) {
-                        atomicOr(&cnt->err, 2u);
-                        break;
-                    }
-                    const unsigned long long old = atomicCAS(&st.table[pos], kEmptySlot, mine);
-                    if (old == kEmptySlot) break;
-                    pos = (pos + 1) & st.tmask;
+        else if (miss) {
+            const uint64_t idx = s_base + off + __popc(ball & lt_mask);
+            store_key<W>(st.keys, idx, p);
+            st.coef[idx] = (sinv * ph) * v;
+            const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
+            for (uint64_t probes = 0;; ++probes) {
+                if (probes > st.tmask) {
+                    atomicOr(&cnt->err, 2u);
+                    break;
                 }
+                const unsigned long long old = atomicCAS(&st.table[pos], kEmptySlot, mine);
+                if (old == kEmptySlot) break;
+                pos = (pos + 1) & st.tmask;
             }
-            if (ball != 0 && __popc(ball) <= 4) {
-                // Bit-columns of the appended terms (InvertedIndex::append_rows, InvertedIndex.h:178-193);
-                // column bits of terms not yet appended are zero, so OR is enough. Few appends in the
-                // warp: each lane ORs its own bits.
-                if (miss) {
-                    int pop = 0;
-                    const uint32_t bit = 1u << (idx & 31);
-#pragma unroll
-                    for (int w = 0; w < W; ++w) {
-                        pop += __popcll(p[w]);
-                        for (uint64_t x = p[w]; x != 0; x &= x - 1)
-                            atomicOr(st.cols + static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1) *
-                                                   st.cstride + (idx >> 5),
-                                     bit);
-                    }
-                    if (pop & 1) atomicOr(st.cols + static_cast<uint64_t>(64 * W) * st.cstride + (idx >> 5), bit);
-                }
-            }
-            else if (ball != 0) {
-                // Many appends: the warp's indices are consecutive, so they touch at most two column
-                // words; per column the lanes' bits are combined by a warp reduction and OR-ed once.
-                const uint64_t j0 = first >> 5;
-                const uint32_t mybit = miss ? (1u << (idx & 31)) : 0u;
-                const bool upper = miss && ((idx >> 5) != j0);
+            // Bit-columns of the append (InvertedIndex::append_rows, InvertedIndex.h:178-193): a warp with
+            // few appends ORs its lanes' bits here (column bits of terms not yet stored are zero); dense
+            // runs are left to k_columns, which transposes whole 32-term words.
+            if (__popc(ball) <= kSparseAppends) {
                 int pop = 0;
+                const uint32_t bit = 1u << (idx & 31);
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
-                    const uint64_t pk = miss ? p[w] : 0ULL;
-                    pop += __popcll(pk);
-                    uint64_t u = (static_cast<uint64_t>(__reduce_or_sync(0xFFFFFFFFu, static_cast<uint32_t>(pk >> 32)))
-                                  << 32) |
-                                 __reduce_or_sync(0xFFFFFFFFu, static_cast<uint32_t>(pk));
-                    for (; u != 0; u &= u - 1) {
-                        const int b = __ffsll(static_cast<long long>(u)) - 1;
-                        const bool has = (pk >> b) & 1ULL;
-                        const uint32_t r0 = __reduce_or_sync(0xFFFFFFFFu, (has && !upper) ? mybit : 0u);
-                        const uint32_t r1 = __reduce_or_sync(0xFFFFFFFFu, (has && upper) ? mybit : 0u);
-                        if (lane == 0) {
-                            uint32_t *col = st.cols + static_cast<uint64_t>(64 * w + b) * st.cstride;
-                            if (r0) atomicOr(col + j0, r0);
-                            if (r1) atomicOr(col + j0 + 1, r1);
-                        }
-                    }
+                    pop += __popcll(p[w]);
+                    for (uint64_t x = p[w]; x != 0; x &= x - 1)
+                        atomicOr(st.cols + static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1) *
+                                               st.cstride + (idx >> 5),
+                                 bit);
                 }
-                const uint32_t r0 = __reduce_or_sync(0xFFFFFFFFu, ((pop & 1) && !upper) ? mybit : 0u);
-                const uint32_t r1 = __reduce_or_sync(0xFFFFFFFFu, ((pop & 1) && upper) ? mybit : 0u);
-                if (lane == 0) {
-                    uint32_t *col = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
-                    if (r0) atomicOr(col + j0, r0);
-                    if (r1) atomicOr(col + j0 + 1, r1);
-                }
+                if (pop & 1) atomicOr(st.cols + static_cast<uint64_t>(64 * W) * st.cstride + (idx >> 5), bit);
+            }
+            else if (__popc(ball & lt_mask) == 0) {
+                atomicOr(&cnt->cols_dirty, 1u);
             }
         }
         __syncthreads();
@@ -495,7 +470,7 @@ template <int W>
 __global__ void __launch_bounds__(kBlock) k_columns(Store st, const Counters *__restrict__ cnt, uint64_t lo,
                                                      uint64_t hi, int from_counters) {
     if (from_counters) {
-        if (cnt->stall != kNoStall) return;
+        if (cnt->stall != kNoStall || cnt->cols_dirty == 0) return; // sparse appends were written by k_resolve
         lo = cnt->n0;
         hi = cnt->n;
     }

@@ -69,6 +69,38 @@ class MonomialPropagator:
             raise ValueError("propagate() needs a circuit with bound parameters.")
         self._simulator.propagate([list(m) for m in monos], mapping, g, params, only_rotate_len_k)
 
+    def build_graph(self, circuit: Circuit, *, seed_parameters=None, only_rotate_len_k: int | None = None) -> None:
+        """Keep the circuit's truncation structure, built at ``seed_parameters`` (default: the circuit's
+        own), for evaluation at other parameters (``monomial_propagator.py:201-255``)."""
+        self._check_circuit(circuit)
+        gates = self._circuit_gates(circuit)
+        monos, g, mapping, gidx = expand_monomials(gates, circuit.resolved_mapping, self._system_size)
+        seed = circuit.parameters if seed_parameters is None else seed_parameters
+        self._simulator.build_graph([list(m) for m in monos], mapping, g, gidx, self._bind(seed) or None,
+                                    only_rotate_len_k)
+        self._n_params = circuit.n_parameters
+
+    @property
+    def n_parameters(self) -> int:
+        return getattr(self, "_n_params", 0)
+
+    def graph_layers(self) -> int:
+        return self._simulator.graph_layers()
+
+    def gradient(self, parameters=None):
+        return self.expectation_value_and_gradient(parameters)[1]
+
+    def expectation_value_functional(self):
+        """A callable ``parameters -> <O>`` over the stored graph (or the current operator)."""
+        return lambda parameters=None: self.expectation_value(parameters)
+
+    def expectation_value_and_gradient_functional(self):
+        return lambda parameters=None: self.expectation_value_and_gradient(parameters)
+
+    expval_functional = expectation_value_functional
+    expval_and_grad_functional = expectation_value_and_gradient_functional
+    grad = gradient
+
     def expectation_value(self, parameters=None) -> float:
         return self._simulator.expectation_value(self._bind(parameters))
 

@@ -200,6 +200,11 @@ def batch_ising50(n_instances: int = 256, seed: int = 99, min_depth: int = 4, ma
 
 BY_NAME = {"line20": line20, "ising100": ising100, "hubbard6x6": hubbard6x6}
 
+#: sum over gates of the terms present when the gate is applied (term-gate updates) for the default
+#: seeds, as counted by the oracle and the reference engine; the GPU engine's per-gate counters must sum
+#: to the same numbers (tests/test_gpu_parity.py). The reference's timing arm divides by these.
+TERM_GATE_UPDATES = {"line20": 694_230, "hubbard6x6": 3_416_554_382, "ising100": 107_553_458_845}
+
 
 def from_circuit(name: str, operator, circuit, *, cutoff: int, cutoff_type: str = "length",
                  lower_atol: float | None = None, upper_atol: float | None = None) -> Workload:

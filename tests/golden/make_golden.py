@@ -9,6 +9,8 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
   sum and sum of squares of the coefficients in key order;
 * ``grad_<workload>.npz`` -- the reference's gradient of the frozen-structure surrogate (graph built with
   the same parameters, then ``expectation_value_and_gradient``), per parameter;
+* ``graph_<workload>.npz`` -- the reference's frozen graph (built at the workload's parameters) replayed
+  at shifted parameters: expectation and gradient there;
 * ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
   replayed graph;
 * ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
@@ -63,6 +65,8 @@ GRADS = [
     ("ising100_L600", W.ising100, 600),
     ("ising50_d2", lambda: W.ising50(2), None),
 ]
+
+GRAPHS = [("hubbard6x6_L300", W.hubbard6x6, 300), ("ising100_L600", W.ising100, 600)]
 
 # The full 100-qubit, 5600-angle circuit: the reference's analytic gradient drifts for the angles it
 # reaches last in its reverse sweep (angle 5202: -1.2165 analytic vs 4.6e-5 by finite differences of the
@@ -140,6 +144,22 @@ def main(reference_root: str = "/root/reference") -> None:
         np.savez_compressed(os.path.join(HERE, f"fd_{name}.npz"), expectation=np.float64(ev0), idx=idx, fd=fd,
                             h=np.float64(h))
         print("fd", name, ev0, float(np.abs(fd).max()))
+    # Frozen-structure replay at new parameters: the reference's graph built at the workload's parameters,
+    # then expectation_value_and_gradient at theta' = theta + 0.05 * N(0, 1) (seed 77): graph_<name>.npz.
+    for name, make, L in GRAPHS:
+        wl = make()
+        n_layers = wl.n_layers if L is None else L
+        eng = oracle.RefEngine(wl)
+        eng.propagate(n_layers=L, build_graph=True)
+        n_params = int(wl.param_map[:n_layers].max()) + 1
+        theta = wl.params[:n_params]
+        shifted = theta + 0.05 * np.random.default_rng(77).standard_normal(n_params)
+        ev, grad, _ = eng.expectation_and_gradient(shifted)
+        ev0 = eng.expectation(theta)
+        eng.close()
+        np.savez_compressed(os.path.join(HERE, f"graph_{name}.npz"), expectation=np.float64(ev),
+                            expectation_build=np.float64(ev0), grad=grad, params=shifted, n_layers=np.int64(n_layers))
+        print("graph", name, ev0, ev, float(np.abs(grad).max()))
     # Parameter-shift gradient of the 20-qubit line circuit from the reference's replayed graph: each
     # replayed layer is affine in (cos 2 g theta, sin 2 g theta), so E(theta + s e_p) - E(theta - s e_p)
     # with s = pi / (4 |g|) times |g| is the exact derivative of the frozen surrogate (one layer per

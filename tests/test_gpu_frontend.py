@@ -86,3 +86,37 @@ def test_pauli_from_circuit_matches_oracle():
     evolved = pp.evolved_operator(atol=0.0)
     # atol = 0 keeps every stored term plus the (zero) identity core term, as the reference does
     assert len(evolved.terms) == pp.size() + 1 and evolved.terms[Pauli("")] == 0.0
+
+
+@pytest.mark.parametrize("name", ["ref_rx_rz_ry_rz_exact", "ref_random_exact"])
+def test_graph_exact_energy_and_gradient(name):
+    """build_graph + replayed functionals (tests/test_infinite_cutoff.py:39-108 of the reference): the
+    exact energy and gradient at infinite cutoff, and central finite differences at cutoff 4."""
+    g = golden.load(name)
+    wl = golden.fixture_workload(g, name)
+    circuit = Circuit.from_dense_arrays(wl.gate_slots, wl.gen_coeffs, wl.param_map, wl.num_modes, wl.params,
+                                        wl.initial_state)
+    op = MajoranaOperator(wl.observable, wl.num_modes)
+    mp = MajoranaPropagator(op, wl.initial_state, cutoff=2 * wl.num_modes)
+    mp.build_graph(circuit)
+    assert np.isclose(mp.expval_functional()(wl.params), float(g["exact_energy"]), atol=1e-12)
+    ev, grad = mp.expval_and_grad(wl.params)
+    assert np.isclose(ev, float(g["exact_energy"]), atol=1e-12)
+    assert np.allclose(grad, g["exact_gradient"], atol=1e-10)
+
+    prng = np.random.default_rng(0)
+    mp4 = MajoranaPropagator(op, wl.initial_state, cutoff=4)
+    mp4.build_graph(circuit)
+    fn = mp4.expval_functional()
+    xk = prng.random(size=len(wl.params))
+    eps = 1e-6
+    fd = np.zeros_like(xk)
+    for i in range(len(xk)):
+        old = xk[i]
+        xk[i] = old + eps
+        ep = fn(xk)
+        xk[i] = old - eps
+        em = fn(xk)
+        fd[i] = (ep - em) / (2 * eps)
+        xk[i] = old
+    assert np.allclose(mp4.grad(xk), fd, atol=1e-6)

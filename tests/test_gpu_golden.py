@@ -73,7 +73,8 @@ def test_reset_and_resident_circuit_with_new_angles():
     first = eng.expectation()
     eng.reset()
     eng.propagate_circuit(circ)
-    assert eng.expectation() == first
+    # appends land in a run-dependent order, so the sum may differ in the last bits
+    assert abs(eng.expectation() - first) <= 1e-14 * max(1.0, abs(first))
     p2 = wl.params * 1.1
     circ.set_angles(wl.angles(p2)[:L])
     eng.reset()

@@ -56,3 +56,13 @@ def test_hubbard_prefix():
 
 def test_ising50_depth5():
     compare(W.ising50(5))
+
+
+@pytest.mark.parametrize("name", ["line20", "hubbard6x6", "ising100"])
+def test_term_gate_update_counts(name):
+    """The engine's per-gate counters sum to the oracle's term-gate update count of each bench workload."""
+    wl = W.BY_NAME[name]()
+    eng = _native.engine_for(wl)
+    eng.propagate(wl.gen_words(), wl.angles())
+    assert eng.gate_stats().term_gate_updates == W.TERM_GATE_UPDATES[name]
+    eng.close()

@@ -73,3 +73,10 @@ def test_analytic_one_gate_truncation(cutoff, upper_atol, lower_atol, kept):
         assert got[(0, 2, 3, 4)] == pytest.approx(0.8660254037844386, abs=1e-15)
     else:
         assert (0, 2, 3, 4) not in got
+
+
+def test_term_gate_update_count_of_the_line_circuit():
+    from monoprop_b200.workloads import TERM_GATE_UPDATES
+
+    r = oracle.run_port(W.line20())
+    assert int(r.counts[:, 0].sum()) == TERM_GATE_UPDATES["line20"]
