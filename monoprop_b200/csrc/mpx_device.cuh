@@ -46,8 +46,6 @@ struct Counters {
     unsigned long long n0; // term count at the start of the current gate
     uint32_t stall;        // kNoStall, or the step index at which capacity ran out
     uint32_t err;          // nonzero: a bounded probe loop gave up (table inconsistent); results invalid
-    uint32_t cols_dirty;   // this gate appended dense runs whose bit-columns k_columns must write
-    uint32_t pad;
 };
 
 struct StateMask {

@@ -191,7 +191,6 @@ void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t 
     k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
                                                        e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    k_columns<W><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->d_cnt, 0, 0, 1);
     if (ev) cudaEventRecord(ev[3], e->stream);
 }
 
@@ -628,7 +627,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             // One launch for the whole range; a gate that would overflow stalls the rest (no-ops), and the
             // host resumes from it below exactly as after a chunk.
             MPX_CUDA(cudaGraphLaunch(g.exec, e->stream));
-            e->launches += 3 * (hi - lo);
+            e->launches += 2 * (hi - lo);
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[0], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
             MPX_CUDA(cudaEventRecord(e->ev[0], e->stream));
             step = hi;
@@ -646,7 +645,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             for (uint64_t st = step; st < stop; ++st) {
                 gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
             }
-            e->launches += 3 * (stop - step);
+            e->launches += 2 * (stop - step);
             MPX_CUDA(cudaGetLastError());
             const uint64_t slot = chunk_id & 1;
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[slot], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));

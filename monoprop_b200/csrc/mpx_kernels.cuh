@@ -1,16 +1,14 @@
 // mpx_kernels.cuh -- the per-gate kernels of the B200 propagation engine (sm_100a).
 //
-// One Heisenberg gate = three launches over the device term store:
+// One Heisenberg gate = two launches over the device term store:
 //   k_sweep   -- anticommutation test from the generator's bit-columns (|fold| bits per term), fused cos
 //                scaling of the anticommuting coefficients, lower_atol / structural-cutoff / upper_atol
 //                emit gate, rotation phase, leader/follower class; compacts the emitted sine branches into
 //                the query arrays and writes the leader-emitted bitmap.
 //   k_resolve -- one thread per emitted branch: open-addressing lookup of the partner M^G, the
 //                leader/follower rule, the rotation of the pair, or the unique append of the missing partner.
-//   k_columns -- adds the appended terms to the bit-columns when some warp appended a dense run (and
-//                builds them on construction, growth, reset); sparse appends OR their bits in k_resolve.
-//                Transposing whole 32-term words with ballots beats OR-ing bits when a gate appends many
-//                terms, and a launch that finds nothing to do returns at once.
+//              It also ORs the appended terms' bits into the bit-columns.
+//   k_columns -- (re)builds the bit-columns of a range of stored terms (construction, growth, reset).
 // Every coefficient slot is written by exactly one thread per gate (the sine partner map M -> M^G is
 // injective), so no coefficient atomics are needed (layer_build/FusedApply.h:54-56).
 #pragma once
@@ -40,7 +38,7 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
 constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
-constexpr int kSparseAppends = 4;    // appends per warp round up to which k_resolve writes the bit-columns
+constexpr int kBatch = 8;            // chunks per warp whose column scans are issued together
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
 // warp w of block b scans the 1024-term chunks b + grid * (w + warps * i) and owns query region
@@ -73,10 +71,10 @@ template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                    Trunc tr, Tape tp) {
-    __shared__ uint32_t s_anti[kWarps][32];
-    __shared__ uint32_t s_foll[kWarps][32];
-    __shared__ uint32_t s_pfx[kWarps][32];
-    __shared__ uint32_t s_emit[kWarps][32];
+    __shared__ uint32_t s_anti[kWarps][kBatch * 32];
+    __shared__ uint32_t s_foll[kWarps][kBatch * 32];
+    __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
+    __shared__ uint32_t s_emit[kWarps][kBatch * 32];
     __shared__ uint32_t s_red[kWarps][2];
     __shared__ uint32_t s_fold[kMaxFoldCols];
     if (cnt->stall != kNoStall) return;
@@ -87,10 +85,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         if (threadIdx.x == 0) atomicMin(&cnt->stall, step);
         return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        cnt->n0 = n0;
-        cnt->cols_dirty = 0;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n0 = n0;
     const GateDesc &gd = gates[gate];
     const int n_fold = gd.n_fold;
     if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
@@ -114,49 +109,57 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         // Consecutive chunks go to consecutive blocks (chunk = block + grid * (warp + warps * i)): the
         // oldest terms, which carry the largest coefficients and most of the emitted branches, spread
         // over all blocks instead of piling up in the first few, for the sweep and for the resolve.
-        for (uint64_t chunk = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp; chunk < geo.nchunks;
-             chunk += geo.n_warps) {
-            const uint64_t j = chunk * 32 + lane;
-            uint32_t anti = 0, foll = 0;
-            if (j < geo.nwords) {
-                if (n_fold <= kMaxFoldCols) {
-                    // all fold-column loads in flight at once
-                    uint32_t v[kMaxFoldCols];
+        // A warp takes its chunks in batches of kBatch: first the anticommutation masks of the whole
+        // batch (the column loads of all its chunks in flight together), then rounds over the batch's
+        // anticommuting terms in (chunk, lane, bit) order.
+        const uint64_t first = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp;
+        for (uint64_t c0 = first; c0 < geo.nchunks; c0 += static_cast<uint64_t>(kBatch) * geo.n_warps) {
+            const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
+            const int nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+            int total = 0;
+#pragma unroll 2
+            for (int b = 0; b < nb; ++b) {
+                const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+                uint32_t anti = 0, foll = 0;
+                if (j < geo.nwords) {
+                    if (n_fold <= kMaxFoldCols) {
+                        uint32_t v[kMaxFoldCols];
 #pragma unroll
-                    for (int f = 0; f < kMaxFoldCols; ++f)
-                        v[f] = f < n_fold ? st.cols[static_cast<uint64_t>(s_fold[f]) * st.cstride + j] : 0u;
+                        for (int f = 0; f < kMaxFoldCols; ++f)
+                            v[f] = f < n_fold ? st.cols[static_cast<uint64_t>(s_fold[f]) * st.cstride + j] : 0u;
 #pragma unroll
-                    for (int f = 0; f < kMaxFoldCols; ++f) anti ^= v[f];
-                }
-                else {
+                        for (int f = 0; f < kMaxFoldCols; ++f) anti ^= v[f];
+                    }
+                    else {
 #pragma unroll
-                    for (int w = 0; w < W; ++w) {
-                        for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
-                            const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
-                            anti ^= st.cols[c * st.cstride + j];
+                        for (int w = 0; w < W; ++w) {
+                            for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
+                                const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
+                                anti ^= st.cols[c * st.cstride + j];
+                            }
                         }
                     }
+                    if (gd.g_odd) anti ^= parity[j];
+                    if (j == geo.nwords - 1) anti &= tail;
+                    foll = anti & pivot[j];
                 }
-                if (gd.g_odd) anti ^= parity[j];
-                if (j == geo.nwords - 1) anti &= tail;
-                foll = anti & pivot[j];
-            }
-            const int cnt_l = __popc(anti);
-            int incl = cnt_l;
+                const int cnt_l = __popc(anti);
+                int incl = cnt_l;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                if (lane >= o) incl += t;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                s_anti[warp][b * 32 + lane] = anti;
+                s_foll[warp][b * 32 + lane] = foll;
+                s_pfx[warp][b * 32 + lane] = static_cast<uint32_t>(total + incl - cnt_l);
+                s_emit[warp][b * 32 + lane] = 0;
+                total += __shfl_sync(0xFFFFFFFFu, incl, 31);
             }
-            const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-            s_anti[warp][lane] = anti;
-            s_foll[warp][lane] = foll;
-            s_pfx[warp][lane] = static_cast<uint32_t>(incl - cnt_l);
-            s_emit[warp][lane] = 0;
             __syncwarp();
             // Rounds of up to 32 * kPrefetch anticommuting terms: every lane first issues the coefficient
             // loads of its kPrefetch terms (independent random accesses in flight together), then
-            // processes them one by one.
+            // processes them one by one. loc = (batch word) * 32 + bit.
             for (int k = 0; k < total; k += 32 * kPrefetch) {
                 int loc[kPrefetch];
                 double vv[kPrefetch];
@@ -166,14 +169,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                     loc[r] = -1;
                     vv[r] = 0.0;
                     if (idx < total) {
-                        int lo = 0, hi = 32;
+                        int lo = 0, hi = nb * 32;
                         while (hi - lo > 1) {
                             const int mid = (lo + hi) >> 1;
                             if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
                             else hi = mid;
                         }
                         loc[r] = lo * 32 + nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
-                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(loc[r])];
+                        const uint64_t chunk = c0 + static_cast<uint64_t>(lo >> 5) * geo.n_warps;
+                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(loc[r] & 1023)];
                     }
                 }
 #pragma unroll
@@ -181,11 +185,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                     if (k + 32 * r >= total) break; // warp-uniform
                     const int l = loc[r];
                     const double v = vv[r];
-                    const uint64_t term = chunk * 1024 + static_cast<uint64_t>(l < 0 ? 0 : l);
+                    const int word = l < 0 ? 0 : (l >> 5); // batch word: chunk (word >> 5), lane (word & 31)
+                    const uint64_t term = (c0 + static_cast<uint64_t>(word >> 5) * geo.n_warps) * 1024 +
+                                          static_cast<uint64_t>(l < 0 ? 0 : (l & 1023));
                     bool emit = false, follower = false;
                     int phase = 0;
                     if (l >= 0) {
-                        follower = (s_foll[warp][l >> 5] >> (l & 31)) & 1u;
+                        follower = (s_foll[warp][word] >> (l & 31)) & 1u;
                         st.coef[term] = v * cosv;
                         if (cos_zero) sc.aux[term] = v;
                         if constexpr (REPLAY) {
@@ -218,14 +224,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                         sc.q_src[q] = static_cast<uint32_t>(term);
                         sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
                         sc.q_val[q] = v;
-                        if (!follower) atomicOr(&s_emit[warp][l >> 5], 1u << (l & 31));
+                        if (!follower) atomicOr(&s_emit[warp][word], 1u << (l & 31));
                     }
                     qcount += __popc(eb);
                 }
             }
             anti_count += static_cast<uint32_t>(total);
             __syncwarp();
-            if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][lane];
+            for (int b = 0; b < nb; ++b) {
+                const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+                if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][b * 32 + lane];
+            }
             __syncwarp();
         }
     }
@@ -438,10 +447,10 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 if (old == kEmptySlot) break;
                 pos = (pos + 1) & st.tmask;
             }
-            // Bit-columns of the append (InvertedIndex::append_rows, InvertedIndex.h:178-193): a warp with
-            // few appends ORs its lanes' bits here (column bits of terms not yet stored are zero); dense
-            // runs are left to k_columns, which transposes whole 32-term words.
-            if (__popc(ball) <= kSparseAppends) {
+            // Bit-columns of the append (InvertedIndex::append_rows, InvertedIndex.h:178-193): each lane ORs
+            // its term's bits (column bits of terms not yet stored are zero). On an append-heavy gate this
+            // costs about what a separate ballot transposition does, and nothing extra on sparse ones.
+            {
                 int pop = 0;
                 const uint32_t bit = 1u << (idx & 31);
 #pragma unroll
@@ -453,9 +462,6 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                                  bit);
                 }
                 if (pop & 1) atomicOr(st.cols + static_cast<uint64_t>(64 * W) * st.cstride + (idx >> 5), bit);
-            }
-            else if (__popc(ball & lt_mask) == 0) {
-                atomicOr(&cnt->cols_dirty, 1u);
             }
         }
         __syncthreads();
@@ -470,7 +476,7 @@ template <int W>
 __global__ void __launch_bounds__(kBlock) k_columns(Store st, const Counters *__restrict__ cnt, uint64_t lo,
                                                      uint64_t hi, int from_counters) {
     if (from_counters) {
-        if (cnt->stall != kNoStall || cnt->cols_dirty == 0) return; // sparse appends were written by k_resolve
+        if (cnt->stall != kNoStall) return;
         lo = cnt->n0;
         hi = cnt->n;
     }
