@@ -191,6 +191,9 @@ def main() -> None:
 
     from monoprop_b200 import workloads as WL
 
+    if args.workload == "batch" and args.impl == "reference":
+        batch_reference(args)
+        return
     wl = WL.BY_NAME[args.workload]()
     rank, world, local, dist = _dist()
     cores = args.cpu_partitions or _cpu_threads()
@@ -340,6 +343,9 @@ def main() -> None:
                 "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms),
                                        "k_columns": statistics.mean(columns_ms)},
                 "path_bytes_per_step": path_bytes,
+                # the sweep's binding resource: random 32-byte DRAM sectors (each anticommuting coefficient is
+                # read and written once, each emitted term's key row read), per second of sweep time
+                "random_sectors_per_s": float((2 * anti + np.ceil(W / 4) * emitted).sum()) / (statistics.mean(sweep_ms) * 1e-3),
                 "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
     # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on the
     # 8 M-term profiling case, see profiles/) scaled to this workload's algorithmic bytes per launch.
@@ -399,7 +405,14 @@ def batch_bench(args) -> None:
 
     rank, world, local, dist = _dist()
     torch.cuda.set_device(local)
-    batch = WL.batch_ising50(args.batch_instances)
+    if dist is not None:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    full = WL.batch_ising50(args.batch_instances)
+    # instances are independent: rank r takes every world-th one (no data-path collective)
+    batch = full[rank::world]
     seg = 4 * 135
     run_batch(batch[-4:], BatchConfig(), gradient=True, segment_gates=seg, device=local)  # warm-up
     tuner = Autotuner(cache_path=os.path.join(ROOT, "gpurun_out", "autotune.json"))
@@ -411,24 +424,60 @@ def batch_bench(args) -> None:
         tuned.append(run_batch(batch, best, gradient=True, segment_gates=seg, device=local))
         default.append(run_batch(batch, BatchConfig(), gradient=True, segment_gates=seg, device=local))
     fwd = run_batch(batch, best, gradient=False, device=local)
-    t_tuned = min(r.seconds for r in tuned)
-    t_default = min(r.seconds for r in default)
-    n = len(batch)
+    dev = torch.device("cuda", local)
+    t_tuned = max_over_ranks(min(r.seconds for r in tuned), dist, dev)
+    t_default = max_over_ranks(min(r.seconds for r in default), dist, dev)
+    t_fwd = max_over_ranks(fwd.seconds, dist, dev)
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    n = len(full)
+    batch = full
     depths = [wl.n_layers // 135 for wl in batch]
     line = {"metric": "<O>+full-gradient/s", "value": n / t_tuned, "unit": "gradients/s", "n_gpus": world,
             "steps": len(tuned), "warmup": 1, "ms_per_step": 1e3 * t_tuned, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuits)",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuits)",
             "config": {"workload": f"batch of {n} 5x10 kicked-Ising instances, depth {min(depths)}..{max(depths)}, "
                                    "Pauli weight <= 8, lower_atol 1e-5, gradient checkpoints every 540 gates",
+                       "parallelism": f"instances split over {world} GPU(s), no collective on the data path",
                        "angles": int(sum(wl.n_layers for wl in batch)),
                        "final_terms_max": int(max(int(x) for x in tuned[0].final_terms))},
             "autotuned": {**best.as_dict(), "seconds": t_tuned, "tuning_seconds": tune_s,
                           "candidates": entry["table"]},
             "default": {**BatchConfig().as_dict(), "seconds": t_default},
-            "forward_only": {"value": n / fwd.seconds, "unit": "expectations/s", "seconds": fwd.seconds},
+            "forward_only": {"value": n / t_fwd, "unit": "expectations/s", "seconds": t_fwd},
             "e2e": {"value": n / t_tuned, "unit": "gradients/s",
                     "h2d_bytes_per_step": int(sum(wl.gen_words().nbytes + wl.angles().nbytes for wl in batch)),
                     "d2h_bytes_per_step": int(sum(8 * (wl.n_layers + 1) for wl in batch))}}
+    print(json.dumps(line), flush=True)
+
+
+def batch_reference(args) -> None:
+    """The reference engine on a bounded, depth-stratified sample of the batch (forward propagate of each
+    sampled instance on all host threads); the rate is instances per second."""
+    import oracle
+
+    from monoprop_b200 import workloads as WL
+
+    rank, world, _, _ = _dist()
+    if rank != 0:
+        return
+    full = WL.batch_ising50(args.batch_instances)
+    order = sorted(range(len(full)), key=lambda i: full[i].n_layers)
+    sample = [full[i] for i in order[:: max(1, len(order) // 4)][:4]]
+    cores = args.cpu_partitions or _cpu_threads()
+    secs = [time_reference(wl, 1, 0, cores)["seconds"][0] for wl in sample]
+    v = len(sample) / sum(secs)
+    line = {"metric": "<O>/s (forward)", "value": v, "unit": "expectations/s", "n_gpus": args.gpus, "steps": 1,
+            "warmup": 0, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuits)",
+            "config": {"workload": f"batch of {len(full)} 5x10 kicked-Ising instances (depth-stratified sample of "
+                                   f"{len(sample)}: depths {[wl.n_layers // 135 for wl in sample]})"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "expectations/s", "cores": cores, "kind": "reference",
+                             "sample": f"{len(sample)} instances, one forward propagate each"},
+            "e2e": {"value": v, "unit": "expectations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 

@@ -183,6 +183,14 @@ MPX_API mpx_status mpx_graph_expectation(mpx_engine *e, const mpx_circuit *c, do
 MPX_API mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation,
                                       double *grad_angles);
 
+/* Pair log of a gradient forward pass (mpx_adjoint_forward, mpx_graph_build). The forward pass records
+ * every gate's rotated and appended pairs (source, partner, phase), so that mpx_adjoint_backward replays
+ * its segments without the hash resolve and mpx_graph_build needs no second pass; if the log overflows,
+ * both replay the resolve instead (same results). capacity < 0: sized from the previous pass, at most half
+ * the free device memory (default); 0: no log; > 0: that many records (9 bytes each). The reference's
+ * graph build records the same pairs (MonomialPropagator.inl:620-690); this knob replaces nothing there. */
+MPX_API mpx_status mpx_set_pair_log(mpx_engine *e, int64_t capacity);
+
 /* Per-kernel timing. With profiling on, the sweep, resolve and column-append launches of every gate are
  * bracketed by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms)
  * for the last propagate call. The reference has no device kernels; this replaces nothing there (its

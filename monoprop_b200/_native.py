@@ -23,7 +23,7 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_graph_build", "mpx_graph_expectation",
-            "mpx_graph_gradient", "mpx_set_profiling", "mpx_kernel_times",
+            "mpx_graph_gradient", "mpx_set_pair_log", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run")
 
@@ -83,6 +83,7 @@ def load() -> C.CDLL:
             "mpx_graph_build": (st, [vp, vp, u64, C.POINTER(C.c_double)]),
             "mpx_graph_expectation": (st, [vp, vp, C.POINTER(C.c_double)]),
             "mpx_graph_gradient": (st, [vp, vp, u64, C.POINTER(C.c_double), vp]),
+            "mpx_set_pair_log": (st, [vp, C.c_int64]),
             "mpx_set_profiling": (st, [vp, C.c_int32]),
             "mpx_kernel_times": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(u64)]),
@@ -275,6 +276,10 @@ class Engine:
         g = np.zeros(max(circuit.n_layers, 1), dtype=np.float64)
         self._check(self.lib.mpx_graph_gradient(self.h, circuit.h, int(segment_gates), C.byref(out), _p(g)))
         return out.value, g[: circuit.n_layers]
+
+    def set_pair_log(self, capacity: int) -> None:
+        """Pair log of the gradient forward pass: < 0 automatic, 0 off, > 0 that many records."""
+        self._check(self.lib.mpx_set_pair_log(self.h, int(capacity)))
 
     def set_profiling(self, on: bool) -> None:
         self._check(self.lib.mpx_set_profiling(self.h, int(bool(on))))

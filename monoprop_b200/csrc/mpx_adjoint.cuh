@@ -43,6 +43,13 @@ struct Tape {
     uint32_t *w_anti;          // forward pass: [n_steps][sweep warps] anticommuting terms per warp
     const uint64_t *u_off;     // replay: [steps of the segment][sweep warps] first undo record per warp
     uint64_t u_off_step0;      // step of u_off's first row
+    // forward pass of a gradient: every rotated or appended pair (src, tgt, phase | appended) in step order,
+    // r_begin[step] its first record; records past r_cap are counted but not written
+    uint32_t *r_src;
+    uint32_t *r_tgt;
+    int8_t *r_code;
+    uint64_t *r_begin;
+    uint64_t r_cap;
 };
 
 // Per step of a segment: exclusive prefix over the sweep warps' anticommuting counts -> undo offsets

@@ -46,6 +46,7 @@ struct Counters {
     unsigned long long n0; // term count at the start of the current gate
     uint32_t stall;        // kNoStall, or the step index at which capacity ran out
     uint32_t err;          // nonzero: a bounded probe loop gave up (table inconsistent); results invalid
+    unsigned long long rec_total; // pair records written by a recording forward pass (may exceed capacity)
 };
 
 struct StateMask {
@@ -66,15 +67,14 @@ struct Store {
     uint64_t cap;     // term capacity
 };
 
-// Emitted sine branches of the current gate. Warp w of the sweep grid owns the query region
-// [w * stride, w * stride + q_count[w]), stride = (chunks per warp) * 1024 >= the terms it scans, so no
-// two warps ever contend for a slot or a counter; the resolve block b takes the regions of the sweep
-// block b's warps.
+// Emitted sine branches of the current gate. Block b of the sweep grid owns the query region
+// [b * warps * stride, b * warps * stride + blk_q[b]), stride = (chunks per warp) * 1024, at least the
+// terms its warps scan, so blocks never contend for a slot or a counter; the resolve block b takes
+// the region of the sweep block b.
 struct Scratch {
     uint32_t *q_src;     // source term index
     uint8_t *q_flag;     // bit0 follower, bits1-2 phase code (0:+1, 1:-1, 2:0)
     double *q_val;       // pre-gate source coefficient v_src
-    uint32_t *q_count;   // [grid * warps per block] queries per warp region
     uint32_t *blk_anti;  // [grid] anticommuting terms per sweep block
     uint32_t *blk_q;     // [grid] queries per sweep block
     uint32_t *emit_bits; // leader-emitted flags, one bit per term (column-word layout)

@@ -56,6 +56,12 @@ struct AdjointState {
     uint64_t n_final = 0;
     std::vector<uint64_t> stats; // [L][4] n_g, a_g, e_g, (unused) per step
     uint32_t *w_anti = nullptr;   // [L][sweep warps] anticommuting terms per sweep warp and step
+    // pairs recorded by the forward pass (valid when rec_ok: the log did not overflow)
+    uint32_t *r_src = nullptr, *r_tgt = nullptr;
+    int8_t *r_code = nullptr;
+    uint64_t *r_begin = nullptr;
+    uint64_t r_total = 0;
+    bool rec_ok = false;
 };
 
 // A frozen structure (the surrogate "graph" of the reference's variational loop): every gate's rotated
@@ -114,10 +120,14 @@ struct mpx_engine {
     struct GraphEntry {
         uint64_t circuit_id, lo, hi, gen;
         const uint32_t *w_anti;
+        const uint32_t *r_src;
+        uint64_t r_cap;
         cudaGraphExec_t exec;
     };
     std::vector<GraphEntry> graphs;
     uint64_t store_gen = 0;
+    uint64_t rec_hint = 0;
+    int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity // pair records the last recording forward pass needed (sizes the next log)
     bool use_graphs = true;
     bool small_path = true; // run small stores in one shared-memory block (mpx_small.cuh)
     std::string err;
@@ -622,7 +632,8 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     bool replayed = false;
     if (graphable) {
         for (const auto &g : e->graphs) {
-            if (g.circuit_id != cd.id || g.lo != lo || g.hi != hi || g.gen != gen0 || g.w_anti != e->fwd_tape.w_anti)
+            if (g.circuit_id != cd.id || g.lo != lo || g.hi != hi || g.gen != gen0 || g.w_anti != e->fwd_tape.w_anti ||
+                g.r_src != e->fwd_tape.r_src || g.r_cap != e->fwd_tape.r_cap)
                 continue;
             // One launch for the whole range; a gate that would overflow stalls the rest (no-ops), and the
             // host resumes from it below exactly as after a chunk.
@@ -668,6 +679,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 fresh.n0 = n;
                 fresh.stall = kNoStall;
                 fresh.err = snap.err;
+                fresh.rec_total = snap.rec_total; // a recording pass keeps its log offsets
                 MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &fresh, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
                 MPX_CUDA(cudaStreamSynchronize(e->stream));
                 step = at;
@@ -700,7 +712,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 cudaGraphExecDestroy(e->graphs.front().exec);
                 e->graphs.erase(e->graphs.begin());
             }
-            e->graphs.push_back({cd.id, lo, hi, gen0, e->fwd_tape.w_anti, exec});
+            e->graphs.push_back({cd.id, lo, hi, gen0, e->fwd_tape.w_anti, e->fwd_tape.r_src, e->fwd_tape.r_cap, exec});
         }
         else {
             e->use_graphs = false; // capture unavailable here: keep issuing kernels directly
@@ -767,6 +779,10 @@ void free_adjoint(mpx_engine *e) {
         dev_free(e, p);
     dev_free(e, e->adj.final_coef);
     dev_free(e, e->adj.w_anti);
+    dev_free(e, e->adj.r_src);
+    dev_free(e, e->adj.r_tgt);
+    dev_free(e, e->adj.r_code);
+    dev_free(e, e->adj.r_begin);
     e->adj = AdjointState{};
     e->fwd_tape = Tape{};
 }
@@ -785,6 +801,30 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
     const uint64_t n_warps = static_cast<uint64_t>(e->grid) * kWarps;
     MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.w_anti), std::max<uint64_t>(L, 1) * n_warps * sizeof(uint32_t)));
     e->fwd_tape.w_anti = e->adj.w_anti;
+    // The pair log: sized by what the last recording pass needed (or the store capacity), checked after.
+    if (e->pair_log != 0) {
+        uint64_t r_cap = e->pair_log > 0 ? static_cast<uint64_t>(e->pair_log)
+                                         : std::max<uint64_t>({e->rec_hint + e->rec_hint / 4, e->st.cap, 1ULL << 16});
+        // at most half of the free device memory, so that the store, the checkpoints and the backward
+        // tape still fit (9 bytes per record)
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) r_cap = std::min<uint64_t>(r_cap, free_b / 2 / 9);
+        cudaError_t ce = dev_alloc(e, reinterpret_cast<void **>(&e->adj.r_src), r_cap * sizeof(uint32_t));
+        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->adj.r_tgt), r_cap * sizeof(uint32_t));
+        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->adj.r_code), r_cap * sizeof(int8_t));
+        if (ce == cudaSuccess)
+            ce = dev_alloc(e, reinterpret_cast<void **>(&e->adj.r_begin), std::max<uint64_t>(L, 1) * sizeof(uint64_t));
+        if (ce == cudaSuccess) {
+            e->fwd_tape.r_src = e->adj.r_src;
+            e->fwd_tape.r_tgt = e->adj.r_tgt;
+            e->fwd_tape.r_code = e->adj.r_code;
+            e->fwd_tape.r_begin = e->adj.r_begin;
+            e->fwd_tape.r_cap = r_cap;
+        }
+        else {
+            cudaGetLastError(); // no room for a log: the backward pass replays with the streaming kernels
+        }
+    }
     for (uint64_t lo = 0; lo < L; lo += K) {
         double *ck = nullptr;
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double)));
@@ -798,6 +838,11 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
             return s;
         }
         n = e->h_cnt->n;
+    }
+    if (e->fwd_tape.r_src != nullptr) {
+        e->adj.r_total = e->h_cnt->rec_total;
+        e->adj.rec_ok = e->adj.r_total <= e->fwd_tape.r_cap;
+        e->rec_hint = std::max(e->rec_hint, e->adj.r_total);
     }
     e->fwd_tape = Tape{};
     MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(n, 1) * sizeof(double)));
@@ -961,6 +1006,38 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
 
 // ----- frozen structure (graph) -----------------------------------------------------------------------
 
+// The pairs a recording forward pass logged, as a frozen structure over the adjoint state's arrays (the
+// view owns only p_count, filled here).
+mpx_status recorded_view(mpx_engine *eng, FrozenGraph &v) {
+    mpx_engine *e = eng;
+    const AdjointState &A = e->adj;
+    const uint64_t L = A.L;
+    std::vector<uint64_t> begin(L);
+    if (L > 0)
+        MPX_CUDA(cudaMemcpyAsync(begin.data(), A.r_begin, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    v = FrozenGraph{};
+    v.L = L;
+    v.n_final = A.n_final;
+    v.src = A.r_src;
+    v.tgt = A.r_tgt;
+    v.code = A.r_code;
+    v.p_begin = A.r_begin;
+    v.w_anti = A.w_anti;
+    v.n0.resize(L);
+    v.anti.resize(L);
+    v.count.resize(L);
+    for (uint64_t st = 0; st < L; ++st) {
+        v.n0[st] = A.stats[4 * st];
+        v.anti[st] = A.stats[4 * st + 1];
+        v.count[st] = (st + 1 < L ? begin[st + 1] : A.r_total) - begin[st];
+    }
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&v.p_count), std::max<uint64_t>(L, 1) * sizeof(unsigned long long)));
+    if (L > 0)
+        MPX_CUDA(cudaMemcpyAsync(v.p_count, v.count.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+    return MPX_OK;
+}
+
 void free_graph(mpx_engine *e) {
     FrozenGraph &g = e->fg;
     for (void *p : {static_cast<void *>(g.src), static_cast<void *>(g.tgt), static_cast<void *>(g.code),
@@ -980,6 +1057,22 @@ mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_g
     AdjointState &A = e->adj;
     FrozenGraph &g = e->fg;
     const uint64_t L = A.L, nf = A.n_final;
+    if (A.rec_ok) {
+        // The forward pass logged every gate's pairs: the graph takes the log over, no replay needed.
+        s = recorded_view(e, g);
+        if (s != MPX_OK) return s;
+        g.circuit_id = cd.id;
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&g.done), std::max<uint64_t>((nf + 31) / 32, 4) * sizeof(uint32_t)));
+        MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+        A.r_src = nullptr;
+        A.r_tgt = nullptr;
+        A.r_code = nullptr;
+        A.r_begin = nullptr;
+        A.w_anti = nullptr;
+        free_adjoint(e);
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+        return MPX_OK;
+    }
     const size_t S = A.seg_lo.size();
     std::vector<uint64_t> begin(L), u_base(L), n_next(L);
     uint64_t total_e = 0, u_max = 1;
@@ -1227,7 +1320,6 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.q_count), e->grid * kWarps * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_anti), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_q), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
@@ -1470,7 +1562,14 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
                                         "with no propagation in between");
     MPX_CUDA(cudaSetDevice(e->device));
     if (c->n == 0) return MPX_OK;
-    return adjoint_backward(e, *c, grad_angles);
+    if (!e->adj.rec_ok) return adjoint_backward(e, *c, grad_angles);
+    // The forward pass recorded every gate's pairs: replay the segments with the frozen kernels.
+    FrozenGraph view;
+    mpx_status s = recorded_view(e, view);
+    if (s != MPX_OK) return s;
+    s = adjoint_backward(e, *c, grad_angles, &view);
+    dev_free(e, view.p_count);
+    return s;
 }
 
 mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation) {
@@ -1514,6 +1613,12 @@ mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segm
     e->adj.w_anti = nullptr; // owned by the graph
     free_adjoint(e);
     return s;
+}
+
+mpx_status mpx_set_pair_log(mpx_engine *e, int64_t capacity) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    e->pair_log = capacity;
+    return MPX_OK;
 }
 
 mpx_status mpx_set_profiling(mpx_engine *e, int32_t on) {
@@ -1567,7 +1672,6 @@ void mpx_destroy(mpx_engine *e) {
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
     for (auto &ev : e->pev) cudaEventDestroy(ev);
-    cudaFree(e->sc.q_count);
     cudaFree(e->sc.blk_anti);
     cudaFree(e->sc.blk_q);
     cudaFree(e->d_partial);

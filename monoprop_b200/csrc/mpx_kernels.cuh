@@ -41,8 +41,8 @@ constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coeff
 constexpr int kBatch = 8;            // chunks per warp whose column scans are issued together
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
-// warp w of block b scans the 1024-term chunks b + grid * (w + warps * i) and owns query region
-// b * warps + w.
+// warp w of block b scans the 1024-term chunks b + grid * (w + warps * i); block b owns the query
+// region [b * warps * stride, (b + 1) * warps * stride), at least as many slots as its warps scan terms.
 struct SweepGeometry {
     uint64_t nwords, nchunks, stride;
     uint32_t n_warps;
@@ -58,15 +58,17 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 }
 
 // Fused anticommutation scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
-// Each warp owns chunks of 1024 terms (32 column words). The anticommutation bit of 32 terms at once is
-// the XOR of the generator's fold columns (Pauli pair_swap(G), Majorana G, plus the |M|-parity column
-// for odd |G|): only |fold| bits per term are read, not the 8W-byte key. The anticommuting terms of the
-// chunk are then spread over the 32 lanes (prefix sums + popcount bisection); each is cos-scaled, and
+// Warps scan chunks of 1024 terms (32 column words). The anticommutation bit of 32 terms at once is the
+// XOR of the generator's fold columns (Pauli pair_swap(G), Majorana G, plus the |M|-parity column for
+// odd |G|): only |fold| bits per term are read, not the 8W-byte key. The anticommuting terms are then
+// shared out over all the block's threads, whichever warp's chunk holds them: anticommuting terms
+// cluster in index ranges (the appends of one gate tend to anticommute with the next gate), and a warp
+// left alone with a dense chunk would hold its whole block at the end. Each term is cos-scaled, and
 // only those that pass the lower_atol gate load their key row to build the partner M^G, run the
-// structural cutoff / upper_atol rescue and the rotation phase. Emitted branches go to the warp's own
-// query region; nothing is counted through a shared global counter. With a tape, the warp's
-// anticommuting count is saved per step (forward pass of a gradient) and, in REPLAY mode, every
-// anticommuting term's index and pre-gate coefficient go to the undo log at the warp's precomputed offset.
+// structural cutoff / upper_atol rescue and the rotation phase. Emitted branches go to the block's own
+// query region (one shared-counter bump per warp and round). With a tape, each warp's anticommuting
+// count is saved per step (forward pass of a gradient) and, in REPLAY mode, every anticommuting term's
+// index and pre-gate coefficient go to the undo log at its chunk-owning warp's precomputed offset.
 template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
@@ -75,7 +77,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     __shared__ uint32_t s_foll[kWarps][kBatch * 32];
     __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
     __shared__ uint32_t s_emit[kWarps][kBatch * 32];
-    __shared__ uint32_t s_red[kWarps][2];
+    __shared__ uint32_t s_wtot[kWarps];     // anticommuting terms of each warp's current batch
+    __shared__ uint32_t s_wpfx[kWarps + 1]; // their exclusive prefix over the block's warps
+    __shared__ uint32_t s_nw[kWarps];       // column words of each warp's current batch
+    __shared__ unsigned long long s_ubase[kWarps]; // REPLAY: each warp's undo-log position
+    __shared__ uint32_t s_qn;               // the block's queries so far
+    __shared__ uint32_t s_red[kWarps];
     __shared__ uint32_t s_fold[kMaxFoldCols];
     if (cnt->stall != kNoStall) return;
     const uint64_t n0 = cnt->n;
@@ -85,18 +92,24 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         if (threadIdx.x == 0) atomicMin(&cnt->stall, step);
         return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n0 = n0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt->n0 = n0;
+        if (!REPLAY && tp.r_begin != nullptr) tp.r_begin[step] = cnt->rec_total;
+    }
     const GateDesc &gd = gates[gate];
     const int n_fold = gd.n_fold;
+    const SweepGeometry geo = sweep_geometry(n0);
     if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
+    if (threadIdx.x == 0) s_qn = 0;
+    if constexpr (REPLAY) {
+        if (threadIdx.x < kWarps)
+            s_ubase[threadIdx.x] = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * geo.n_warps +
+                                            blockIdx.x * kWarps + threadIdx.x];
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const SweepGeometry geo = sweep_geometry(n0);
-    const uint32_t wg = blockIdx.x * kWarps + warp;
-    uint32_t anti_count = 0, qcount = 0;
-    uint64_t ubase = 0;
-    if constexpr (REPLAY) ubase = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * geo.n_warps + wg];
+    uint32_t anti_count = 0;
     if (!gd.empty && n0 != 0) {
         const double cosv = gd.cosv, sinabs = gd.abs_sin;
         const bool cos_zero = gd.cos_zero != 0;
@@ -104,18 +117,21 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(gd.pivot_col) * st.cstride;
         const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
         const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
-        const uint64_t qbase = static_cast<uint64_t>(wg) * geo.stride;
+        const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
+        const uint64_t span = static_cast<uint64_t>(kBatch) * geo.n_warps;
 
-        // Consecutive chunks go to consecutive blocks (chunk = block + grid * (warp + warps * i)): the
-        // oldest terms, which carry the largest coefficients and most of the emitted branches, spread
-        // over all blocks instead of piling up in the first few, for the sweep and for the resolve.
-        // A warp takes its chunks in batches of kBatch: first the anticommutation masks of the whole
-        // batch (the column loads of all its chunks in flight together), then rounds over the batch's
-        // anticommuting terms in (chunk, lane, bit) order.
-        const uint64_t first = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp;
-        for (uint64_t c0 = first; c0 < geo.nchunks; c0 += static_cast<uint64_t>(kBatch) * geo.n_warps) {
-            const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
-            const int nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+        // Consecutive chunks go to consecutive blocks (warp w of block b takes chunks
+        // b + grid * (w + warps * i)), so dense index ranges spread over all blocks. Each warp takes its
+        // chunks in batches of kBatch (the column loads of the whole batch in flight together); per block
+        // iteration, the anticommuting terms of the block's batches form one list in (warp, chunk, lane,
+        // bit) order, dealt out in rounds of kBlock * kPrefetch.
+        for (uint64_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
+            const uint64_t c0 = it0 + static_cast<uint64_t>(gridDim.x) * warp;
+            int nb = 0;
+            if (c0 < geo.nchunks) {
+                const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
+                nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+            }
             int total = 0;
 #pragma unroll 2
             for (int b = 0; b < nb; ++b) {
@@ -156,46 +172,72 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                 s_emit[warp][b * 32 + lane] = 0;
                 total += __shfl_sync(0xFFFFFFFFu, incl, 31);
             }
-            __syncwarp();
-            // Rounds of up to 32 * kPrefetch anticommuting terms: every lane first issues the coefficient
-            // loads of its kPrefetch terms (independent random accesses in flight together), then
-            // processes them one by one. loc = (batch word) * 32 + bit.
-            for (int k = 0; k < total; k += 32 * kPrefetch) {
+            if (lane == 0) {
+                s_wtot[warp] = static_cast<uint32_t>(total);
+                s_nw[warp] = static_cast<uint32_t>(nb * 32);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t acc = 0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) {
+                    s_wpfx[w] = acc;
+                    acc += s_wtot[w];
+                }
+                s_wpfx[kWarps] = acc;
+            }
+            __syncthreads();
+            const int btotal = static_cast<int>(s_wpfx[kWarps]);
+            // Rounds of up to kBlock * kPrefetch anticommuting terms: every thread first issues the
+            // coefficient loads of its kPrefetch terms (independent random accesses in flight together),
+            // then processes them one by one. loc = owner * (kBatch * 1024) + (batch word) * 32 + bit.
+            for (int k = 0; k < btotal; k += kBlock * kPrefetch) {
                 int loc[kPrefetch];
                 double vv[kPrefetch];
 #pragma unroll
                 for (int r = 0; r < kPrefetch; ++r) {
-                    const int idx = k + 32 * r + lane;
+                    const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
                     loc[r] = -1;
                     vv[r] = 0.0;
-                    if (idx < total) {
-                        int lo = 0, hi = nb * 32;
+                    if (idx < btotal) {
+                        int ow = 0;
+#pragma unroll
+                        for (int w = 1; w < kWarps; ++w) ow += (static_cast<int>(s_wpfx[w]) <= idx) ? 1 : 0;
+                        const int li = idx - static_cast<int>(s_wpfx[ow]);
+                        int lo = 0, hi = static_cast<int>(s_nw[ow]);
                         while (hi - lo > 1) {
                             const int mid = (lo + hi) >> 1;
-                            if (static_cast<int>(s_pfx[warp][mid]) <= idx) lo = mid;
+                            if (static_cast<int>(s_pfx[ow][mid]) <= li) lo = mid;
                             else hi = mid;
                         }
-                        loc[r] = lo * 32 + nth_set_bit(s_anti[warp][lo], idx - static_cast<int>(s_pfx[warp][lo]));
-                        const uint64_t chunk = c0 + static_cast<uint64_t>(lo >> 5) * geo.n_warps;
-                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(loc[r] & 1023)];
+                        const int l = lo * 32 + nth_set_bit(s_anti[ow][lo], li - static_cast<int>(s_pfx[ow][lo]));
+                        loc[r] = ow * (kBatch * 1024) + l;
+                        const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
+                                               static_cast<uint64_t>(lo >> 5) * geo.n_warps;
+                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(l & 1023)];
                     }
                 }
 #pragma unroll
                 for (int r = 0; r < kPrefetch; ++r) {
-                    if (k + 32 * r >= total) break; // warp-uniform
-                    const int l = loc[r];
+                    if (k + kBlock * r + 32 * warp >= btotal) break; // warp-uniform
+                    const int L = loc[r];
                     const double v = vv[r];
-                    const int word = l < 0 ? 0 : (l >> 5); // batch word: chunk (word >> 5), lane (word & 31)
-                    const uint64_t term = (c0 + static_cast<uint64_t>(word >> 5) * geo.n_warps) * 1024 +
-                                          static_cast<uint64_t>(l < 0 ? 0 : (l & 1023));
+                    const int ow = L < 0 ? 0 : (L / (kBatch * 1024));
+                    const int l = L < 0 ? 0 : (L % (kBatch * 1024));
+                    const int word = l >> 5; // batch word: chunk (word >> 5), lane (word & 31)
+                    const uint64_t term = (it0 + static_cast<uint64_t>(gridDim.x) * ow +
+                                           static_cast<uint64_t>(word >> 5) * geo.n_warps) * 1024 +
+                                          static_cast<uint64_t>(l & 1023);
                     bool emit = false, follower = false;
                     int phase = 0;
-                    if (l >= 0) {
-                        follower = (s_foll[warp][word] >> (l & 31)) & 1u;
+                    if (L >= 0) {
+                        follower = (s_foll[ow][word] >> (l & 31)) & 1u;
                         st.coef[term] = v * cosv;
                         if (cos_zero) sc.aux[term] = v;
                         if constexpr (REPLAY) {
-                            const uint64_t rr = ubase + anti_count + static_cast<uint64_t>(k + 32 * r + lane);
+                            const uint64_t rr = s_ubase[ow] + static_cast<uint64_t>(k + kBlock * r +
+                                                                                     static_cast<int>(threadIdx.x) -
+                                                                                     static_cast<int>(s_wpfx[ow]));
                             tp.u_idx[rr] = static_cast<uint32_t>(term);
                             tp.u_val[rr] = v;
                         }
@@ -219,46 +261,46 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                         }
                     }
                     const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
+                    uint32_t qb = 0;
+                    if (lane == 0 && eb != 0) qb = atomicAdd(&s_qn, static_cast<uint32_t>(__popc(eb)));
+                    qb = __shfl_sync(0xFFFFFFFFu, qb, 0);
                     if (emit) {
-                        const uint64_t q = qbase + qcount + __popc(eb & lt_mask);
+                        const uint64_t q = qbase + qb + __popc(eb & lt_mask);
                         sc.q_src[q] = static_cast<uint32_t>(term);
                         sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
                         sc.q_val[q] = v;
-                        if (!follower) atomicOr(&s_emit[warp][word], 1u << (l & 31));
+                        if (!follower) atomicOr(&s_emit[ow][word], 1u << (l & 31));
                     }
-                    qcount += __popc(eb);
                 }
             }
-            anti_count += static_cast<uint32_t>(total);
-            __syncwarp();
+            __syncthreads(); // every round of this batch is done: the emit bitmaps are final
             for (int b = 0; b < nb; ++b) {
                 const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
                 if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][b * 32 + lane];
+            }
+            anti_count += static_cast<uint32_t>(total);
+            if constexpr (REPLAY) {
+                if (lane == 0) s_ubase[warp] += static_cast<unsigned long long>(total);
             }
             __syncwarp();
         }
     }
     if (lane == 0) {
-        sc.q_count[wg] = qcount;
-        if (tp.w_anti != nullptr && !REPLAY) tp.w_anti[static_cast<uint64_t>(step) * geo.n_warps + wg] = anti_count;
-        s_red[warp][0] = anti_count;
-        s_red[warp][1] = qcount;
+        if (tp.w_anti != nullptr && !REPLAY) tp.w_anti[static_cast<uint64_t>(step) * geo.n_warps + blockIdx.x * kWarps + warp] = anti_count;
+        s_red[warp] = anti_count;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t t = 0, q = 0;
+        uint32_t t = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            t += s_red[w][0];
-            q += s_red[w][1];
-        }
+        for (int w = 0; w < kWarps; ++w) t += s_red[w];
         sc.blk_anti[blockIdx.x] = t;
-        sc.blk_q[blockIdx.x] = q;
+        sc.blk_q[blockIdx.x] = s_qn;
     }
 }
 
 // Partner resolve + rotation apply + append (Engine.h:364-513, FusedApply.h:32-83, MPOperator.h:269-278).
-// Resolve block b processes the query regions of sweep block b's warps, in block-wide rounds; appends
+// Resolve block b processes the query region of sweep block b, in block-wide rounds; appends
 // take one counter bump per round. In REPLAY mode the keys of this gate's appends already exist
 // (indices >= n0, inserted by the forward pass): a partner found there is treated as the append it was,
 // nothing is inserted, and every rotated or appended pair goes to the tape's pair log with both
@@ -268,7 +310,6 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                      uint64_t *__restrict__ stats, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
-    __shared__ uint32_t s_pfx[kWarps + 1];
     __shared__ unsigned long long s_base, s_rbase;
     __shared__ unsigned long long s_sum[2][kWarps];
     if (cnt->stall != kNoStall) return;
@@ -308,19 +349,9 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
         }
     }
     if (gd.empty || n0 == 0) return;
-    if (threadIdx.x < kWarps) warp_cnt[threadIdx.x] = sc.q_count[blockIdx.x * kWarps + threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int w = 0; w < kWarps; ++w) {
-            s_pfx[w] = acc;
-            acc += warp_cnt[w];
-        }
-        s_pfx[kWarps] = acc;
-    }
-    __syncthreads();
-    const uint32_t total = s_pfx[kWarps];
+    const uint32_t total = sc.blk_q[blockIdx.x];
     if (total == 0) return;
+    const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
     uint64_t g[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) g[w] = gd.g[w];
@@ -336,10 +367,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
         int8_t code = 0;
         double v = 0.0, ph = 0.0, vt = 0.0;
         if (k < total) {
-            int r = 0;
-#pragma unroll
-            for (int w = 1; w < kWarps; ++w) r += (s_pfx[w] <= k) ? 1 : 0;
-            const uint64_t q = static_cast<uint64_t>(blockIdx.x * kWarps + r) * geo.stride + (k - s_pfx[r]);
+            const uint64_t q = qbase + k;
             src = sc.q_src[q];
             const uint8_t flag = sc.q_flag[q];
             v = sc.q_val[q];
@@ -399,11 +427,9 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
                     st.coef[src] = __fma_rn(sinv * -ph, vt, st.coef[src]);
                     st.coef[found] = __fma_rn(sinv * ph, v, st.coef[found]);
-                    if constexpr (REPLAY) {
-                        rec = true;
-                        tgt = static_cast<uint32_t>(found);
-                        code = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
-                    }
+                    rec = true; // a rotated pair (recorded in replay mode and by a recording forward pass)
+                    tgt = static_cast<uint32_t>(found);
+                    code = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
                 }
             }
         }
@@ -462,6 +488,33 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                                  bit);
                 }
                 if (pop & 1) atomicOr(st.cols + static_cast<uint64_t>(64 * W) * st.cstride + (idx >> 5), bit);
+            }
+        }
+        if constexpr (!REPLAY) {
+            if (tp.r_src != nullptr) {
+                // recording forward pass: this round's rotated pairs and appends, one counter bump per round
+                const bool has = rec || miss;
+                const uint32_t rb = __ballot_sync(0xFFFFFFFFu, has);
+                __syncthreads();
+                if (lane == 0) warp_cnt[warp] = __popc(rb);
+                __syncthreads();
+                uint32_t roff = 0, rtot = 0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) {
+                    const uint32_t t = warp_cnt[w];
+                    roff += (w < warp) ? t : 0u;
+                    rtot += t;
+                }
+                if (threadIdx.x == 0 && rtot > 0) s_rbase = atomicAdd(&cnt->rec_total, static_cast<unsigned long long>(rtot));
+                __syncthreads();
+                if (has) {
+                    const uint64_t r = s_rbase + roff + __popc(rb & lt_mask);
+                    if (r < tp.r_cap) {
+                        tp.r_src[r] = src;
+                        tp.r_tgt[r] = miss ? static_cast<uint32_t>(s_base + off + __popc(ball & lt_mask)) : tgt;
+                        tp.r_code[r] = static_cast<int8_t>((miss ? 0x10 : 0) | (static_cast<int>(ph) & 0xF));
+                    }
+                }
             }
         }
         __syncthreads();
