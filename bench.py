@@ -346,6 +346,9 @@ def main() -> None:
                 # the sweep's binding resource: random 32-byte DRAM sectors (each anticommuting coefficient is
                 # read and written once, each emitted term's key row read), per second of sweep time
                 "random_sectors_per_s": float((2 * anti + np.ceil(W / 4) * emitted).sum()) / (statistics.mean(sweep_ms) * 1e-3),
+                # per step: anticommuting terms (cos-scaled), emitted sine branches, appended partners
+                "anticommuting_per_step": int(anti.sum()), "emitted_per_step": int(emitted.sum()),
+                "appended_per_step": int(app.sum()),
                 "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
     # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on the
     # 8 M-term profiling case, see profiles/) scaled to this workload's algorithmic bytes per launch.

@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
             v = sc.q_val[q];
             ph = phase_value(static_cast<uint8_t>(flag >> 1));
             uint64_t m[W];
-            load_key<W>(st.keys, src, m);
+            load_key<W>(st.keys, src, m); // mostly an L2 hit: the sweep has just read this row
 #pragma unroll
             for (int w = 0; w < W; ++w) p[w] = m[w] ^ g[w];
             const uint64_t h = key_hash<W>(p);
