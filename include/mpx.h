@@ -200,9 +200,10 @@ MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *res
                                     uint64_t *n_gates);
 
 /* Device memory of all engines on a device comes from one library-owned pool that keeps freed memory
- * mapped for reuse (so creating engines and regrowing stores does not re-map gigabytes each time). This
- * returns the cached, unused part of that pool to the driver. No reference counterpart (the reference
- * is host-only). */
+ * mapped for reuse, and freed blocks of 1 MiB or more are kept whole, per power-of-two size class, for
+ * the next request of that class (so creating engines and regrowing stores does not re-map gigabytes
+ * each time). This hands the kept blocks back to the pool and returns the pool's unused memory to the
+ * driver. No reference counterpart (the reference is host-only). */
 MPX_API mpx_status mpx_trim_device_memory(int32_t device);
 
 MPX_API const char *mpx_last_error(const mpx_engine *e);

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/mpx.h"
@@ -176,19 +177,124 @@ cudaMemPool_t engine_pool(int device) {
     return pool;
 }
 
-cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
-    return cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream);
-}
-
-void dev_free(mpx_engine *e, void *ptr) {
-    if (ptr != nullptr) cudaFreeAsync(ptr, e->stream);
-}
-
 uint64_t next_pow2(uint64_t x) {
     uint64_t p = 1;
     while (p < x) p <<= 1;
     return p;
 }
+
+// Large blocks (>= 1 MiB) are not handed back to the pool when freed but kept, per device and
+// power-of-two size class, for the next request of that class: a store that regrows, or the next
+// engine of the same workload, gets the very same mapped block back. Asking the pool for a multi-GB
+// block instead can cost a second or more when it has to assemble the block from freed pieces. A kept
+// block carries an event recorded on the stream that freed it, which the next user's stream waits on.
+// When an allocation fails, every kept block of the device goes back to the pool and it is retried;
+// mpx_trim_device_memory does the same and then trims the pool.
+struct KeptBlock {
+    void *ptr;
+    cudaEvent_t ready;
+};
+struct BlockCache {
+    std::mutex mu;
+    std::map<std::pair<int, size_t>, std::vector<KeptBlock>> idle; // (device, class) -> blocks
+    std::unordered_map<void *, size_t> live;                        // block -> class, while in use
+};
+BlockCache &block_cache() {
+    static BlockCache *c = new BlockCache; // never destroyed: engines may outlive static destruction
+    return *c;
+}
+constexpr size_t kKeepMin = size_t(1) << 20;
+
+// Returns every kept block of `device` to the pool (the caller has made `device` current).
+void release_kept_blocks(int device) {
+    BlockCache &c = block_cache();
+    std::vector<KeptBlock> out;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        for (auto it = c.idle.begin(); it != c.idle.end();) {
+            if (it->first.first == device) {
+                out.insert(out.end(), it->second.begin(), it->second.end());
+                it = c.idle.erase(it);
+            }
+            else {
+                ++it;
+            }
+        }
+    }
+    for (const KeptBlock &b : out) {
+        cudaEventSynchronize(b.ready);
+        cudaEventDestroy(b.ready);
+        cudaFreeAsync(b.ptr, nullptr);
+    }
+    if (!out.empty()) cudaStreamSynchronize(nullptr);
+    cudaGetLastError();
+}
+
+cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
+    BlockCache &c = block_cache();
+    if (bytes < kKeepMin) {
+        const cudaError_t ce = cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream);
+        if (ce == cudaSuccess) { // an address is never on record as a kept class while it is a small block
+            std::lock_guard<std::mutex> lock(c.mu);
+            c.live.erase(*ptr);
+        }
+        return ce;
+    }
+    const size_t cls = next_pow2(bytes);
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.idle.find({e->device, cls});
+        if (it != c.idle.end() && !it->second.empty()) {
+            const KeptBlock b = it->second.back();
+            it->second.pop_back();
+            c.live[b.ptr] = cls;
+            *ptr = b.ptr;
+            const cudaError_t ce = cudaStreamWaitEvent(e->stream, b.ready, 0);
+            cudaEventDestroy(b.ready);
+            return ce;
+        }
+    }
+    cudaError_t ce = cudaMallocFromPoolAsync(ptr, cls, e->pool, e->stream);
+    if (ce == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        release_kept_blocks(e->device);
+        ce = cudaMallocFromPoolAsync(ptr, cls, e->pool, e->stream);
+    }
+    if (ce == cudaSuccess) {
+        std::lock_guard<std::mutex> lock(c.mu);
+        c.live[*ptr] = cls;
+    }
+    return ce;
+}
+
+// Frees a block from dev_alloc, stream-ordered on `stream` of `device` (the current device). Every block
+// from dev_alloc must come back through here: a block of a kept class freed any other way would leave
+// its class on record for an address the pool may hand out again at another size.
+void dev_release(int device, cudaStream_t stream, void *ptr) {
+    if (ptr == nullptr) return;
+    BlockCache &c = block_cache();
+    size_t cls = 0;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.live.find(ptr);
+        if (it != c.live.end()) {
+            cls = it->second;
+            c.live.erase(it);
+        }
+    }
+    cudaEvent_t ev = nullptr;
+    if (cls == 0 || cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(ev, stream) != cudaSuccess) {
+        cudaGetLastError();
+        if (ev != nullptr) cudaEventDestroy(ev);
+        cudaFreeAsync(ptr, stream);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.idle[{device, cls}].push_back({ptr, ev});
+}
+
+void dev_free(mpx_engine *e, void *ptr) { dev_release(e->device, e->stream, ptr); }
 
 // ----- kernel dispatch over (W, basis) ------------------------------------------------------------------
 
@@ -376,16 +482,18 @@ BuildFn pick_build(int W) {
 
 // ----- store management ---------------------------------------------------------------------------------
 
+// Store buffers come from the engine's memory pool and go back to it stream-ordered (a plain cudaFree
+// would bypass the pool's bookkeeping, and the next engine would map fresh memory instead of reusing it).
 void free_store(mpx_engine *e) {
-    cudaFree(e->st.keys);
-    cudaFree(e->st.coef);
-    cudaFree(e->st.table);
-    cudaFree(e->st.cols);
-    cudaFree(e->sc.q_src);
-    cudaFree(e->sc.q_flag);
-    cudaFree(e->sc.q_val);
-    cudaFree(e->sc.emit_bits);
-    cudaFree(e->sc.aux);
+    dev_free(e, e->st.keys);
+    dev_free(e, e->st.coef);
+    dev_free(e, e->st.table);
+    dev_free(e, e->st.cols);
+    dev_free(e, e->sc.q_src);
+    dev_free(e, e->sc.q_flag);
+    dev_free(e, e->sc.q_val);
+    dev_free(e, e->sc.emit_bits);
+    dev_free(e, e->sc.aux);
     e->st = Store{};
     e->sc.q_src = nullptr;
     e->sc.q_flag = nullptr;
@@ -549,8 +657,7 @@ mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const doub
     mpx_engine *e = eng;
     std::vector<GateDesc> h(n);
     for (uint64_t l = 0; l < n; ++l) make_desc(e, gen_words + l * e->W, angles[l], h[l]);
-    MPX_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&cd.d_desc), std::max<uint64_t>(n, 1) * sizeof(GateDesc),
-                             e->stream));
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&cd.d_desc), std::max<uint64_t>(n, 1) * sizeof(GateDesc)));
     if (n > 0) {
         MPX_CUDA(cudaMemcpyAsync(cd.d_desc, h.data(), n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));
     }
@@ -1409,8 +1516,10 @@ mpx_status mpx_propagate_circuit(mpx_engine *e, const mpx_circuit *c) {
 void mpx_circuit_destroy(mpx_circuit *c) {
     if (c == nullptr) return;
     if (c->d_desc != nullptr) {
+        // pool memory, returned stream-ordered; the circuit may outlive the stream of the engine that made it
         cudaSetDevice(c->device);
-        cudaFree(c->d_desc);
+        dev_release(c->device, nullptr, c->d_desc);
+        cudaStreamSynchronize(nullptr);
     }
     delete c;
 }
@@ -1646,6 +1755,11 @@ mpx_status mpx_trim_device_memory(int32_t device) {
     }
     cudaMemPool_t pool = engine_pool(device);
     if (pool == nullptr) return fail(nullptr, MPX_ERR_CUDA, "cannot create the device memory pool");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    release_kept_blocks(device);
+    cudaSetDevice(prev);
     if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
         cudaGetLastError();
         return fail(nullptr, MPX_ERR_CUDA, "cudaMemPoolTrimTo failed");
@@ -1679,8 +1793,11 @@ void mpx_destroy(mpx_engine *e) {
     cudaFreeHost(e->h_out);
     cudaFree(e->d_init_keys);
     cudaFree(e->d_init_coef);
-    cudaFree(e->d_stats);
-    if (e->stream != nullptr) cudaStreamDestroy(e->stream);
+    dev_free(e, e->d_stats);
+    if (e->stream != nullptr) {
+        cudaStreamSynchronize(e->stream); // the pool frees above are stream-ordered
+        cudaStreamDestroy(e->stream);
+    }
     cudaGetLastError();
     delete e;
 }
