@@ -243,61 +243,6 @@ __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ co
     }
 }
 
-// The other anticommuting terms of one frozen gate (terms < n0 whose fold-column parity is odd): scaled
-// by cos; pair members (done bits, set by k_frozen_pairs) are skipped and their bits cleared. With LOG
-// every anticommuting term's pre-gate value goes to the undo log at the warp's offset, in the same
-// chunk/lane order as the streaming sweep (pair members' entries are never read).
-template <int W, bool LOG>
-__global__ void __launch_bounds__(kBlock) k_frozen_scan(Store st, const GateDesc *__restrict__ gates, uint32_t gate,
-                                                         uint32_t step, uint64_t n0, uint32_t *__restrict__ done,
-                                                         Tape tp) {
-    const GateDesc &gd = gates[gate];
-    if (gd.empty || n0 == 0) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t nwords = (n0 + 31) >> 5, nchunks = (nwords + 31) >> 5;
-    const uint64_t n_warps = static_cast<uint64_t>(gridDim.x) * (kBlock / 32);
-    const uint64_t wg = static_cast<uint64_t>(blockIdx.x) * (kBlock / 32) + warp;
-    const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
-    const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
-    const double C = gd.cosv;
-    uint64_t ubase = 0;
-    if constexpr (LOG) ubase = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * n_warps + wg];
-    uint64_t anti_count = 0;
-    for (uint64_t chunk = blockIdx.x + static_cast<uint64_t>(gridDim.x) * warp; chunk < nchunks; chunk += n_warps) {
-        const uint64_t j = chunk * 32 + lane;
-        uint32_t anti = 0, dn = 0;
-        if (j < nwords) {
-#pragma unroll
-            for (int w = 0; w < W; ++w)
-                for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1)
-                    anti ^= st.cols[static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1) * st.cstride + j];
-            if (gd.g_odd) anti ^= parity[j];
-            if (j == nwords - 1) anti &= tail;
-            dn = done[j];
-            if (dn) done[j] = 0;
-        }
-        // prefix of the lanes' counts: the undo order is (chunk, lane, bit), as in the sweep
-        const int cnt_l = __popc(anti);
-        int incl = cnt_l;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        int r = incl - cnt_l;
-        for (uint32_t a = anti; a != 0; a &= a - 1, ++r) {
-            const int bit = __ffs(a) - 1;
-            const uint64_t i = j * 32 + bit;
-            const double v = st.coef[i];
-            if constexpr (LOG) {
-                tp.u_idx[ubase + anti_count + r] = static_cast<uint32_t>(i);
-                tp.u_val[ubase + anti_count + r] = v;
-            }
-            if (!((dn >> bit) & 1u)) st.coef[i] = v * C;
-        }
-        anti_count += static_cast<uint64_t>(total);
-    }
-}
+// k_frozen_scan, the other half of a frozen gate, shares the sweep's chunk dealing (mpx_kernels.cuh).
 
 }  // namespace mpx

@@ -299,6 +299,155 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     }
 }
 
+// The other anticommuting terms of one frozen gate (terms < n0 whose fold-column parity is odd) are
+// scaled by cos; pair members (done bits, set by k_frozen_pairs) are skipped and their bits cleared.
+// Chunk ownership, batching and the block-wide dealing of the anticommuting terms are the sweep's, so
+// each sweep warp's terms are the ones it counted in the forward pass. With LOG every anticommuting
+// term's pre-gate value goes to the undo log from its chunk-owning warp's offset (pair members' entries
+// are never read).
+template <int W, bool LOG>
+__global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
+    k_frozen_scan(Store st, const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step, uint64_t n0,
+                  uint32_t *__restrict__ done, Tape tp) {
+    __shared__ uint32_t s_anti[kWarps][kBatch * 32];
+    __shared__ uint32_t s_done[kWarps][kBatch * 32];
+    __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
+    __shared__ uint32_t s_wtot[kWarps];
+    __shared__ uint32_t s_wpfx[kWarps + 1];
+    __shared__ uint32_t s_nw[kWarps];
+    __shared__ unsigned long long s_ubase[kWarps];
+    __shared__ uint32_t s_fold[kMaxFoldCols];
+    const GateDesc &gd = gates[gate];
+    if (gd.empty || n0 == 0) return;
+    const int n_fold = gd.n_fold;
+    const SweepGeometry geo = sweep_geometry(n0);
+    if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
+    if constexpr (LOG) {
+        if (threadIdx.x < kWarps)
+            s_ubase[threadIdx.x] = tp.u_off[(static_cast<uint64_t>(step) - tp.u_off_step0) * geo.n_warps +
+                                            blockIdx.x * kWarps + threadIdx.x];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double C = gd.cosv;
+    const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
+    const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
+    const uint64_t span = static_cast<uint64_t>(kBatch) * geo.n_warps;
+    for (uint64_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
+        const uint64_t c0 = it0 + static_cast<uint64_t>(gridDim.x) * warp;
+        int nb = 0;
+        if (c0 < geo.nchunks) {
+            const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
+            nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+        }
+        int total = 0;
+#pragma unroll 2
+        for (int b = 0; b < nb; ++b) {
+            const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+            uint32_t anti = 0, dn = 0;
+            if (j < geo.nwords) {
+                if (n_fold <= kMaxFoldCols) {
+                    uint32_t v[kMaxFoldCols];
+#pragma unroll
+                    for (int f = 0; f < kMaxFoldCols; ++f)
+                        v[f] = f < n_fold ? st.cols[static_cast<uint64_t>(s_fold[f]) * st.cstride + j] : 0u;
+#pragma unroll
+                    for (int f = 0; f < kMaxFoldCols; ++f) anti ^= v[f];
+                }
+                else {
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        for (uint64_t x = gd.fold[w]; x != 0; x &= x - 1) {
+                            const uint64_t c = static_cast<uint64_t>(64 * w + __ffsll(static_cast<long long>(x)) - 1);
+                            anti ^= st.cols[c * st.cstride + j];
+                        }
+                    }
+                }
+                if (gd.g_odd) anti ^= parity[j];
+                if (j == geo.nwords - 1) anti &= tail;
+                dn = done[j];
+                if (dn) done[j] = 0;
+            }
+            const int cnt_l = __popc(anti);
+            int incl = cnt_l;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            s_anti[warp][b * 32 + lane] = anti;
+            s_done[warp][b * 32 + lane] = dn;
+            s_pfx[warp][b * 32 + lane] = static_cast<uint32_t>(total + incl - cnt_l);
+            total += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        }
+        if (lane == 0) {
+            s_wtot[warp] = static_cast<uint32_t>(total);
+            s_nw[warp] = static_cast<uint32_t>(nb * 32);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                s_wpfx[w] = acc;
+                acc += s_wtot[w];
+            }
+            s_wpfx[kWarps] = acc;
+        }
+        __syncthreads();
+        const int btotal = static_cast<int>(s_wpfx[kWarps]);
+        for (int k = 0; k < btotal; k += kBlock * kPrefetch) {
+            uint64_t term[kPrefetch];
+            double vv[kPrefetch];
+            int own[kPrefetch];
+            bool skip[kPrefetch];
+#pragma unroll
+            for (int r = 0; r < kPrefetch; ++r) {
+                const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
+                own[r] = -1;
+                term[r] = 0;
+                vv[r] = 0.0;
+                skip[r] = true;
+                if (idx < btotal) {
+                    int ow = 0;
+#pragma unroll
+                    for (int w = 1; w < kWarps; ++w) ow += (static_cast<int>(s_wpfx[w]) <= idx) ? 1 : 0;
+                    const int li = idx - static_cast<int>(s_wpfx[ow]);
+                    int lo = 0, hi = static_cast<int>(s_nw[ow]);
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (static_cast<int>(s_pfx[ow][mid]) <= li) lo = mid;
+                        else hi = mid;
+                    }
+                    const int bit = nth_set_bit(s_anti[ow][lo], li - static_cast<int>(s_pfx[ow][lo]));
+                    const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
+                                           static_cast<uint64_t>(lo >> 5) * geo.n_warps;
+                    own[r] = ow;
+                    term[r] = chunk * 1024 + static_cast<uint64_t>(lo & 31) * 32 + bit;
+                    skip[r] = (s_done[ow][lo] >> bit) & 1u;
+                    vv[r] = st.coef[term[r]];
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kPrefetch; ++r) {
+                if (own[r] < 0) continue;
+                if constexpr (LOG) {
+                    const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
+                    const uint64_t rr = s_ubase[own[r]] + static_cast<uint64_t>(idx - static_cast<int>(s_wpfx[own[r]]));
+                    tp.u_idx[rr] = static_cast<uint32_t>(term[r]);
+                    tp.u_val[rr] = vv[r];
+                }
+                if (!skip[r]) st.coef[term[r]] = vv[r] * C;
+            }
+        }
+        __syncthreads(); // the lists of this batch are consumed
+        if constexpr (LOG) {
+            if (lane == 0) s_ubase[warp] += static_cast<unsigned long long>(total);
+        }
+        __syncwarp();
+    }
+}
+
 // Partner resolve + rotation apply + append (Engine.h:364-513, FusedApply.h:32-83, MPOperator.h:269-278).
 // Resolve block b processes the query region of sweep block b, in block-wide rounds; appends
 // take one counter bump per round. In REPLAY mode the keys of this gate's appends already exist
