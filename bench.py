@@ -279,13 +279,12 @@ def main() -> None:
     launches = eng.launch_count() - launches0
     # Per-kernel device times from the same number of steps again, each kernel launch bracketed by CUDA
     # events on the engine stream (the events themselves cost time, so these steps are not the value).
-    sweep_ms, resolve_ms, columns_ms = [], [], []
+    sweep_ms, resolve_ms = [], []
     for _ in range(args.steps):
         one_step(True)
-        s_ms, r_ms, c_ms, _ = eng.kernel_times()
+        s_ms, r_ms, _, _ = eng.kernel_times()
         sweep_ms.append(s_ms)
         resolve_ms.append(r_ms)
-        columns_ms.append(c_ms)
     total_ms = max_over_ranks(sum(ms), dist, dev)
     ms_per_step = total_ms / args.steps
     value = updates * world / (ms_per_step * 1e-3)
@@ -340,8 +339,7 @@ def main() -> None:
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "traffic": None, "algorithmic_bytes_per_launch": sweep_bytes / wl.n_layers,
                 "avg_launch_us": sweep_avg_s / wl.n_layers * 1e6,
-                "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms),
-                                       "k_columns": statistics.mean(columns_ms)},
+                "kernel_ms_per_step": {"k_sweep": statistics.mean(sweep_ms), "k_resolve": statistics.mean(resolve_ms)},
                 "path_bytes_per_step": path_bytes,
                 # the sweep's binding resource: random 32-byte DRAM sectors (each anticommuting coefficient is
                 # read and written once, each emitted term's key row read), per second of sweep time

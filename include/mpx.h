@@ -191,9 +191,10 @@ MPX_API mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint6
  * graph build records the same pairs (MonomialPropagator.inl:620-690); this knob replaces nothing there. */
 MPX_API mpx_status mpx_set_pair_log(mpx_engine *e, int64_t capacity);
 
-/* Per-kernel timing. With profiling on, the sweep, resolve and column-append launches of every gate are
- * bracketed by CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms)
- * for the last propagate call. The reference has no device kernels; this replaces nothing there (its
+/* Per-kernel timing. With profiling on, the sweep and resolve launches of every gate are bracketed by
+ * CUDA events on the engine stream; mpx_kernel_times returns their summed device time (ms) for the last
+ * propagate call. columns_ms is 0: no per-gate column launch remains (the resolve ORs the appended
+ * terms' bit-columns). The reference has no device kernels; this replaces nothing there (its
  * closest counterpart is the per-layer wall time the bench harness records, benches/bench_models.py). */
 MPX_API mpx_status mpx_set_profiling(mpx_engine *e, int32_t on);
 MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *resolve_ms, double *columns_ms,

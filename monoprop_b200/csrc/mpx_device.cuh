@@ -75,7 +75,6 @@ struct Scratch {
     uint32_t *q_src;     // source term index
     uint8_t *q_flag;     // bit0 follower, bits1-2 phase code (0:+1, 1:-1, 2:0)
     double *q_val;       // pre-gate source coefficient v_src
-    uint32_t *blk_anti;  // [grid] anticommuting terms per sweep block
     uint32_t *blk_q;     // [grid] queries per sweep block
     uint32_t *emit_bits; // leader-emitted flags, one bit per term (column-word layout)
     double *aux;         // pre-gate coefficients, used only for cos == 0 gates

@@ -302,20 +302,19 @@ template <int W, int B>
 void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
     cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape);
+    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape,
+                                                     e->d_stats);
     if (ev) cudaEventRecord(ev[1], e->stream);
-    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
-                                                       e->fwd_tape);
+    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
-    if (ev) cudaEventRecord(ev[3], e->stream);
 }
 
 // A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends.
 template <int W, int B>
 void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
-    k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
-    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->d_stats,
-                                                             tp);
+    k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp,
+                                                           e->d_stats);
+    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, tp);
     k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
 }
 
@@ -387,10 +386,16 @@ void launch_expect(mpx_engine *e) {
 
 // Hash table and bit-columns of terms [lo, hi).
 template <int W>
-void launch_build(mpx_engine *e, uint64_t lo, uint64_t hi) {
+void launch_table(mpx_engine *e, uint64_t lo, uint64_t hi) {
     if (hi <= lo) return;
     const uint64_t blocks = std::min<uint64_t>((hi - lo + 255) / 256, static_cast<uint64_t>(e->grid) * 4);
     k_build_table<W><<<static_cast<unsigned>(blocks), 256, 0, e->stream>>>(e->st, e->d_cnt, lo, hi);
+}
+
+template <int W>
+void launch_build(mpx_engine *e, uint64_t lo, uint64_t hi) {
+    if (hi <= lo) return;
+    launch_table<W>(e, lo, hi);
     const uint64_t cblocks = std::min<uint64_t>((hi - lo + 32 * kBlock - 1) / (32 * kBlock) + 1,
                                                 static_cast<uint64_t>(e->grid));
     k_columns<W><<<static_cast<unsigned>(cblocks), kBlock, 0, e->stream>>>(e->st, e->d_cnt, lo, hi, 0);
@@ -465,6 +470,18 @@ AdjInitFn pick_adj_init(int W, int basis) {
     case 6: return adj_init_fn<6>(basis);
     case 7: return adj_init_fn<7>(basis);
     default: return adj_init_fn<8>(basis);
+    }
+}
+BuildFn pick_table(int W) {
+    switch (W) {
+    case 1: return &launch_table<1>;
+    case 2: return &launch_table<2>;
+    case 3: return &launch_table<3>;
+    case 4: return &launch_table<4>;
+    case 5: return &launch_table<5>;
+    case 6: return &launch_table<6>;
+    case 7: return &launch_table<7>;
+    default: return &launch_table<8>;
     }
 }
 BuildFn pick_build(int W) {
@@ -549,10 +566,18 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
         cudaGetLastError();
         return fail(eng, MPX_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(ce));
     }
+    // Bit-column words of the kept terms are copied as they are (the bits of terms not yet stored are
+    // zero in them); the words above start at zero, for the appends to OR into.
+    const uint64_t wk = std::min<uint64_t>((n_keep + 31) / 32, cstride);
     if (n_keep > 0) {
         MPX_CUDA(cudaMemcpyAsync(keys, e->st.keys, n_keep * W * sizeof(uint64_t), cudaMemcpyDeviceToDevice, e->stream));
         MPX_CUDA(cudaMemcpyAsync(coef, e->st.coef, n_keep * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+        MPX_CUDA(cudaMemcpy2DAsync(cols, cstride * sizeof(uint32_t), e->st.cols, e->st.cstride * sizeof(uint32_t),
+                                   wk * sizeof(uint32_t), 64 * W + 1, cudaMemcpyDeviceToDevice, e->stream));
     }
+    if (wk < cstride)
+        MPX_CUDA(cudaMemset2DAsync(cols + wk, cstride * sizeof(uint32_t), 0, (cstride - wk) * sizeof(uint32_t),
+                                   64 * W + 1, e->stream));
     dev_free(e, e->st.keys);
     dev_free(e, e->st.coef);
     dev_free(e, e->st.table);
@@ -572,10 +597,8 @@ mpx_status alloc_store(mpx_engine *eng, uint64_t cap, uint64_t n_keep) {
     nsc.q_cap = q_cap;
     e->sc = nsc;
     MPX_CUDA(cudaMemsetAsync(table, 0xFF, tcap * sizeof(unsigned long long), e->stream));
-    // column bits of terms not yet stored must be zero (appends OR theirs in)
-    MPX_CUDA(cudaMemsetAsync(cols, 0, (64 * W + 1) * cstride * sizeof(uint32_t), e->stream));
-    pick_build(W)(e, 0, n_keep);
-    e->launches += n_keep > 0 ? 2 : 0;
+    pick_table(W)(e, 0, n_keep);
+    e->launches += n_keep > 0 ? 1 : 0;
     MPX_CUDA(cudaGetLastError());
     return MPX_OK;
 }
@@ -682,6 +705,8 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     if (L == 0) return MPX_OK;
     mpx_status s = ensure_stats(e, L);
     if (s != MPX_OK) return s;
+    // the sweeps add their blocks' counts into the per-gate counters of the range
+    MPX_CUDA(cudaMemsetAsync(e->d_stats + 4 * lo, 0, 4 * (hi - lo) * sizeof(uint64_t), e->stream));
     if (cd.any_cos_zero && !e->aux_on) {
         clear_graphs(e);
         e->aux_on = true;
@@ -778,8 +803,11 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 MPX_CUDA(cudaStreamSynchronize(e->stream));
                 const uint64_t at = snap.stall;
                 const uint64_t n = e->h_snap[pending_slot].n;
-                // room for the worst case of the stalled gate (2n) with headroom, at least doubling
-                s = alloc_store(e, std::max<uint64_t>(3 * n, 2 * e->st.cap), n);
+                // room for the worst case of the stalled gate (2n) with headroom: four times the capacity
+                // (fewer regrowths), or, if that does not fit, at least double
+                const uint64_t cap0 = e->st.cap;
+                s = alloc_store(e, std::max<uint64_t>(3 * n, 4 * cap0), n);
+                if (s == MPX_ERR_NOMEM) s = alloc_store(e, std::max<uint64_t>(3 * n, 2 * cap0), n);
                 if (s != MPX_OK) return s;
                 Counters fresh{};
                 fresh.n = n;
@@ -832,7 +860,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             float a = 0.f, b = 0.f, c = 0.f;
             MPX_CUDA(cudaEventElapsedTime(&a, e->pev[4 * st], e->pev[4 * st + 1]));
             MPX_CUDA(cudaEventElapsedTime(&b, e->pev[4 * st + 1], e->pev[4 * st + 2]));
-            MPX_CUDA(cudaEventElapsedTime(&c, e->pev[4 * st + 2], e->pev[4 * st + 3]));
+            c = 0.0f; // no per-gate column launch: the resolve ORs the appended terms' bits
             e->t_sweep_ms += a;
             e->t_resolve_ms += b;
             e->t_columns_ms += c;
@@ -1427,7 +1455,6 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_anti), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_q), e->grid * sizeof(uint32_t));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
     if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_out), sizeof(double));
@@ -1786,7 +1813,6 @@ void mpx_destroy(mpx_engine *e) {
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
     for (auto &ev : e->pev) cudaEventDestroy(ev);
-    cudaFree(e->sc.blk_anti);
     cudaFree(e->sc.blk_q);
     cudaFree(e->d_partial);
     cudaFree(e->d_out);

@@ -72,7 +72,7 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
-                                                   Trunc tr, Tape tp) {
+                                                   Trunc tr, Tape tp, uint64_t *__restrict__ stats) {
     __shared__ uint32_t s_anti[kWarps][kBatch * 32];
     __shared__ uint32_t s_foll[kWarps][kBatch * 32];
     __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
@@ -94,7 +94,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         cnt->n0 = n0;
-        if (!REPLAY && tp.r_begin != nullptr) tp.r_begin[step] = cnt->rec_total;
+        if constexpr (!REPLAY) {
+            stats[4 * static_cast<uint64_t>(step)] = n0;
+            if (tp.r_begin != nullptr) tp.r_begin[step] = cnt->rec_total;
+        }
     }
     const GateDesc &gd = gates[gate];
     const int n_fold = gd.n_fold;
@@ -294,8 +297,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
         uint32_t t = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) t += s_red[w];
-        sc.blk_anti[blockIdx.x] = t;
         sc.blk_q[blockIdx.x] = s_qn;
+        if constexpr (!REPLAY) {
+            // per-gate counters for the host (a_g, e_g; zeroed before the range): integer sums, any order
+            auto *ctr = reinterpret_cast<unsigned long long *>(stats + 4 * static_cast<uint64_t>(step));
+            if (t != 0) atomicAdd(ctr + 1, static_cast<unsigned long long>(t));
+            if (s_qn != 0) atomicAdd(ctr + 2, static_cast<unsigned long long>(s_qn));
+        }
     }
 }
 
@@ -457,46 +465,15 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
 template <int W, int BASIS, bool REPLAY = false>
 __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
-                                                     uint64_t *__restrict__ stats, Tape tp) {
+                                                     Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
     __shared__ unsigned long long s_base, s_rbase;
-    __shared__ unsigned long long s_sum[2][kWarps];
     if (cnt->stall != kNoStall) return;
     const uint64_t n0 = cnt->n0;
     const GateDesc &gd = gates[gate];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const SweepGeometry geo = sweep_geometry(n0);
-    if (blockIdx.x == 0) {
-        // per-gate counters for the host: n_g, a_g, e_g (fixed-order sums)
-        unsigned long long a = 0, e = 0;
-        if (!gd.empty && n0 != 0) {
-            for (uint32_t b = threadIdx.x; b < gridDim.x; b += kBlock) {
-                a += sc.blk_anti[b];
-                e += sc.blk_q[b];
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xFFFFFFFFu, a, o);
-            e += __shfl_down_sync(0xFFFFFFFFu, e, o);
-        }
-        if (lane == 0) {
-            s_sum[0][warp] = a;
-            s_sum[1][warp] = e;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long ta = 0, te = 0;
-            for (int w = 0; w < kWarps; ++w) {
-                ta += s_sum[0][w];
-                te += s_sum[1][w];
-            }
-            stats[4 * static_cast<uint64_t>(step) + 0] = n0;
-            stats[4 * static_cast<uint64_t>(step) + 1] = ta;
-            stats[4 * static_cast<uint64_t>(step) + 2] = te;
-        }
-    }
     if (gd.empty || n0 == 0) return;
     const uint32_t total = sc.blk_q[blockIdx.x];
     if (total == 0) return;
@@ -670,49 +647,75 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
     }
 }
 
-// Writes the bit-columns of terms [lo, hi): one warp per 32-term column word, one ballot per key bit.
-// A word that starts below lo already holds valid bits for the terms below lo (and zeros above) and is
-// OR-ed; every other word is assigned whole (zeros above hi included). With from_counters the range is
-// the current gate's appends [n0, n).
+// Writes the bit-columns of terms [lo, hi). A warp takes 8 consecutive column words (256 terms) at a
+// time: for each key word, 64 ballots per 32 terms build the 64 columns' words in shared memory, which
+// then go out as whole 32-byte sectors (8 words of one column per 8 lanes) instead of 4-byte pieces of
+// 64W + 1 different columns. A word that starts below lo already holds valid bits for the terms below lo
+// (and zeros above) and is OR-ed; words outside [lo, hi) are not touched; every other word is assigned
+// whole (zeros above hi included). With from_counters the range is the current gate's appends [n0, n).
 template <int W>
 __global__ void __launch_bounds__(kBlock) k_columns(Store st, const Counters *__restrict__ cnt, uint64_t lo,
                                                      uint64_t hi, int from_counters) {
+    __shared__ uint32_t s_col[kWarps][64][8];
     if (from_counters) {
         if (cnt->stall != kNoStall) return;
         lo = cnt->n0;
         hi = cnt->n;
     }
     if (hi <= lo) return;
-    const int lane = threadIdx.x & 31;
-    const uint64_t w1 = (hi + 31) >> 5;
-    for (uint64_t j = (lo >> 5) + (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; j < w1;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x / 32) {
-        const uint64_t i = j * 32 + lane;
-        uint64_t m[W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t w0 = lo >> 5, w1 = (hi + 31) >> 5;
+    const uint64_t g_first = w0 >> 3, g_end = (w1 + 7) >> 3;
+    const uint64_t n_warps = static_cast<uint64_t>(gridDim.x) * kWarps;
+    for (uint64_t grp = g_first + static_cast<uint64_t>(blockIdx.x) * kWarps + warp; grp < g_end; grp += n_warps) {
+        const uint64_t j0 = grp * 8;
+        int pop[8];
 #pragma unroll
-        for (int w = 0; w < W; ++w) m[w] = 0;
-        if (i >= lo && i < hi) load_key<W>(st.keys, i, m);
-        const bool boundary = j * 32 < lo;
-        uint32_t mine[2 * W];
-        int pop = 0;
-#pragma unroll
+        for (int g = 0; g < 8; ++g) pop[g] = 0;
+#pragma unroll 1
         for (int w = 0; w < W; ++w) {
-            pop += __popcll(m[w]);
 #pragma unroll
-            for (int b = 0; b < 64; ++b) {
-                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (m[w] >> b) & 1ULL);
-                if (lane == (b & 31)) mine[2 * w + (b >> 5)] = bal;
+            for (int g = 0; g < 8; ++g) {
+                const uint64_t i = (j0 + g) * 32 + lane;
+                const uint64_t x = (i >= lo && i < hi) ? st.keys[i * W + w] : 0ULL;
+                pop[g] += __popcll(x);
+                uint32_t lo_b = 0, hi_b = 0;
+#pragma unroll
+                for (int b = 0; b < 32; ++b) {
+                    const uint32_t bl = __ballot_sync(0xFFFFFFFFu, (x >> b) & 1ULL);
+                    const uint32_t bh = __ballot_sync(0xFFFFFFFFu, (x >> (b + 32)) & 1ULL);
+                    if (lane == b) {
+                        lo_b = bl;
+                        hi_b = bh;
+                    }
+                }
+                s_col[warp][lane][g] = lo_b;
+                s_col[warp][lane + 32][g] = hi_b;
             }
+            __syncwarp();
+            // 64 columns x 8 words: four columns per instruction, eight lanes per column
+#pragma unroll 4
+            for (int c4 = 0; c4 < 16; ++c4) {
+                const int c = c4 * 4 + (lane >> 3), g = lane & 7;
+                const uint64_t j = j0 + g;
+                if (j >= w0 && j < w1) {
+                    uint32_t *dst = st.cols + static_cast<uint64_t>(64 * w + c) * st.cstride + j;
+                    const uint32_t v = s_col[warp][c][g];
+                    *dst = (j * 32 < lo) ? (*dst | v) : v;
+                }
+            }
+            __syncwarp();
         }
-        const uint32_t par = __ballot_sync(0xFFFFFFFFu, pop & 1);
+        uint32_t par = 0;
 #pragma unroll
-        for (int r = 0; r < 2 * W; ++r) {
-            uint32_t *dst = st.cols + static_cast<uint64_t>(32 * r + lane) * st.cstride + j;
-            *dst = boundary ? (*dst | mine[r]) : mine[r];
+        for (int g = 0; g < 8; ++g) {
+            const uint32_t b = __ballot_sync(0xFFFFFFFFu, pop[g] & 1);
+            if (lane == g) par = b;
         }
-        if (lane == 0) {
+        const uint64_t j = j0 + lane;
+        if (lane < 8 && j >= w0 && j < w1) {
             uint32_t *dst = st.cols + static_cast<uint64_t>(64 * W) * st.cstride + j;
-            *dst = boundary ? (*dst | par) : par;
+            *dst = (j * 32 < lo) ? (*dst | par) : par;
         }
     }
 }
