@@ -118,6 +118,13 @@ MPX_API mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff);
 MPX_API mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value);
 MPX_API mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value);
 
+/* only_rotate_len_k of the next propagate calls (MonomialPropagator::propagate's argument,
+ * MonomialPropagator.inl:696-718; semantics Scan.h:146-157,376-391 and FusedApply.h:46-52): a term with
+ * more than k set slots takes no part in a gate (neither cos-scaled nor emitted), and a partner outside
+ * that set receives its sine term unscaled. k <= 0 clears it; k > 2*num_modes is rejected with the
+ * reference's message. The gradient and graph entry points reject an engine with k set. */
+MPX_API mpx_status mpx_set_only_rotate_len_k(mpx_engine *e, int64_t k);
+
 /* Device pointers of the live store (keys [n][W], coefficients [n]) for in-process consumers such as
  * the torch wrapper; valid until the next mutating call. */
 MPX_API mpx_status mpx_device_view(mpx_engine *e, const uint64_t **keys, double **coefs, uint64_t *n);

@@ -21,7 +21,8 @@ _STATUS = {1: "MPX_ERR_INVALID", 2: "MPX_ERR_CUDA", 3: "MPX_ERR_NOMEM", 4: "MPX_
 #: Every entry point declared in include/mpx.h.
 EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_set_angles", "mpx_propagate_circuit",
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
-            "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol", "mpx_device_view",
+            "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol",
+            "mpx_set_only_rotate_len_k", "mpx_device_view",
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_graph_build", "mpx_graph_expectation",
             "mpx_graph_gradient", "mpx_set_pair_log", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
@@ -75,6 +76,7 @@ def load() -> C.CDLL:
             "mpx_set_cutoff": (st, [vp, C.c_uint32]),
             "mpx_set_lower_atol": (st, [vp, C.c_int32, C.c_double]),
             "mpx_set_upper_atol": (st, [vp, C.c_int32, C.c_double]),
+            "mpx_set_only_rotate_len_k": (st, [vp, C.c_int64]),
             "mpx_device_view": (st, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]),
             "mpx_stream": (st, [vp, C.POINTER(vp)]),
             "mpx_launch_count": (st, [vp, C.POINTER(u64)]),
@@ -235,6 +237,10 @@ class Engine:
 
     def set_upper_atol(self, value: float | None) -> None:
         self._check(self.lib.mpx_set_upper_atol(self.h, int(value is not None), float(value or 0.0)))
+
+    def set_only_rotate_len_k(self, k: int | None) -> None:
+        """only_rotate_len_k of the next propagate calls (None clears it)."""
+        self._check(self.lib.mpx_set_only_rotate_len_k(self.h, 0 if k is None else int(k)))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -7,8 +7,9 @@
 // export of evolved_operator (MonomialPropagator.inl:1099-1127).
 //
 // Scope: the Heisenberg picture -- propagate, and build_graph + expectation_value[_and_gradient](parameters)
-// over the engine's frozen structure (mpx_graph_*). schrodinger_cutoff, basis_change, only_rotate_len_k,
-// graph functionals with paring, contract_partially and MPI communicators raise NotImplementedError.
+// over the engine's frozen structure (mpx_graph_*). schrodinger_cutoff, basis_change, only_rotate_len_k in
+// build_graph, graph functionals with paring, contract_partially and MPI communicators raise
+// NotImplementedError.
 #include <pybind11/complex.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -150,14 +151,24 @@ public:
     void propagate(const std::vector<std::vector<size_t>> &majoranas, const std::vector<size_t> &parameter_mapping,
                    const std::vector<double> &gen_coeffs, const std::vector<double> &parameters,
                    std::optional<unsigned int> only_rotate_len_k) {
-        if (only_rotate_len_k.has_value()) throw NotSupported("only_rotate_len_k: not implemented by the B200 engine");
+        // validate_only_rotate_len_k_ (Validation.cpp:119-128): a runtime_error subclass in the reference
+        if (only_rotate_len_k.has_value() && (*only_rotate_len_k == 0 || *only_rotate_len_k > 2 * logical_))
+            throw PropagatorConfigError("only_rotate_len_k=" + std::to_string(*only_rotate_len_k) +
+                                        " is out of range; must be 0 < k <= 2*num_qubits");
         if (circ_ != nullptr)
             throw GraphStateConflict("propagate() needs no stored graph; this propagator holds one (build_graph)");
         std::vector<uint64_t> words;
         std::vector<double> angles;
         encode_circuit(majoranas, parameter_mapping, gen_coeffs, parameters, words, angles);
-        py::gil_scoped_release nogil;
-        check(mpx_propagate(e_, words.data(), angles.data(), majoranas.size()), e_);
+        check(mpx_set_only_rotate_len_k(e_, only_rotate_len_k.has_value() ? static_cast<int64_t>(*only_rotate_len_k) : 0),
+              e_);
+        mpx_status st;
+        {
+            py::gil_scoped_release nogil;
+            st = mpx_propagate(e_, words.data(), angles.data(), majoranas.size());
+        }
+        mpx_set_only_rotate_len_k(e_, 0);
+        check(st, e_);
     }
 
     // MonomialPropagator<N>::build_graph (MonomialPropagator.inl:620-690): a coefficient-informed build at

@@ -38,6 +38,9 @@ struct Trunc {
     uint32_t cutoff;
     int32_t has_lower, has_upper;
     double lower, upper;
+    // only_rotate_len_k: terms with more than len_k set slots take no part in a gate (Scan.h:146-157)
+    int32_t has_len_k;
+    uint32_t len_k;
 };
 
 // Device counters, one set per engine.

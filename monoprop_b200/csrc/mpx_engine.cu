@@ -302,10 +302,19 @@ template <int W, int B>
 void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
     cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape,
-                                                     e->d_stats);
+    if (e->tr.has_len_k)
+        k_sweep<W, B, false, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
+                                                                      e->fwd_tape, e->d_stats);
+    else
+        k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
+                                                         e->fwd_tape, e->d_stats);
     if (ev) cudaEventRecord(ev[1], e->stream);
-    k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->fwd_tape);
+    if (e->tr.has_len_k)
+        k_resolve<W, B, false, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step,
+                                                                        e->tr, e->fwd_tape);
+    else
+        k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
+                                                           e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
 }
 
@@ -314,7 +323,7 @@ template <int W, int B>
 void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
     k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp,
                                                            e->d_stats);
-    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, tp);
+    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
     k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
 }
 
@@ -707,7 +716,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     if (s != MPX_OK) return s;
     // the sweeps add their blocks' counts into the per-gate counters of the range
     MPX_CUDA(cudaMemsetAsync(e->d_stats + 4 * lo, 0, 4 * (hi - lo) * sizeof(uint64_t), e->stream));
-    if (cd.any_cos_zero && !e->aux_on) {
+    if ((cd.any_cos_zero || e->tr.has_len_k) && !e->aux_on) {
         clear_graphs(e);
         e->aux_on = true;
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->sc.aux), e->st.cap * sizeof(double)));
@@ -727,7 +736,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     uint64_t pending_slot = 0;
     // Small store: run gates in one shared-memory block until the store outgrows it (or the range ends).
     bool used_small = false;
-    if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && e->fwd_tape.w_anti == nullptr &&
+    if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && !e->tr.has_len_k && e->fwd_tape.w_anti == nullptr &&
         hi - lo >= 8) {
         MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
         MPX_CUDA(cudaStreamSynchronize(e->stream));
@@ -1659,6 +1668,18 @@ mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value) {
     return MPX_OK;
 }
 
+mpx_status mpx_set_only_rotate_len_k(mpx_engine *e, int64_t k) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    const int64_t max_k = 2 * static_cast<int64_t>(e->cfg.num_modes);
+    if (k > max_k)
+        return fail(e, MPX_ERR_INVALID, "only_rotate_len_k=" + std::to_string(k) +
+                                            " is out of range; must be 0 < k <= 2*num_qubits");
+    clear_graphs(e);
+    e->tr.has_len_k = k > 0;
+    e->tr.len_k = k > 0 ? static_cast<uint32_t>(k) : 0;
+    return MPX_OK;
+}
+
 mpx_status mpx_device_view(mpx_engine *e, const uint64_t **keys, double **coefs, uint64_t *n) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     if (keys) *keys = e->st.keys;
@@ -1683,6 +1704,8 @@ mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t seg
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    if (e->tr.has_len_k)
+        return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = adjoint_forward(e, *c, segment_gates);
     if (s != MPX_OK) return s;
@@ -1712,6 +1735,8 @@ mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    if (e->tr.has_len_k)
+        return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = graph_build(e, *c, segment_gates);
     if (s != MPX_OK) return s;

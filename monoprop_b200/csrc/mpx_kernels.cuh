@@ -69,7 +69,7 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 // query region (one shared-counter bump per warp and round). With a tape, each warp's anticommuting
 // count is saved per step (forward pass of a gradient) and, in REPLAY mode, every anticommuting term's
 // index and pre-gate coefficient go to the undo log at its chunk-owning warp's precomputed offset.
-template <int W, int BASIS, bool REPLAY = false>
+template <int W, int BASIS, bool REPLAY = false, bool LENK = false>
 __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                    Trunc tr, Tape tp, uint64_t *__restrict__ stats) {
@@ -233,10 +233,21 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                                           static_cast<uint64_t>(l & 1023);
                     bool emit = false, follower = false;
                     int phase = 0;
-                    if (L >= 0) {
+                    bool member = L >= 0;
+                    if (LENK && member) {
+                        // only_rotate_len_k: a term of more than len_k slots is left alone by this gate
+                        // (no cos scaling, no emit); the partner values of the others are kept in `aux`
+                        uint64_t mk[W];
+                        load_key<W>(st.keys, term, mk);
+                        int kp = 0;
+#pragma unroll
+                        for (int w = 0; w < W; ++w) kp += __popcll(mk[w]);
+                        member = kp <= static_cast<int>(tr.len_k);
+                    }
+                    if (member) {
                         follower = (s_foll[ow][word] >> (l & 31)) & 1u;
                         st.coef[term] = v * cosv;
-                        if (cos_zero) sc.aux[term] = v;
+                        if (cos_zero || LENK) sc.aux[term] = v;
                         if constexpr (REPLAY) {
                             const uint64_t rr = s_ubase[ow] + static_cast<uint64_t>(k + kBlock * r +
                                                                                      static_cast<int>(threadIdx.x) -
@@ -462,10 +473,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
 // (indices >= n0, inserted by the forward pass): a partner found there is treated as the append it was,
 // nothing is inserted, and every rotated or appended pair goes to the tape's pair log with both
 // pre-gate coefficients (one counter bump per round).
-template <int W, int BASIS, bool REPLAY = false>
+template <int W, int BASIS, bool REPLAY = false, bool LENK = false>
 __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
-                                                     Tape tp) {
+                                                     Trunc tr, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
     __shared__ unsigned long long s_base, s_rbase;
     if (cnt->stall != kNoStall) return;
@@ -506,6 +517,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
             tag = static_cast<uint32_t>(h >> 32);
             pos = h & st.tmask;
             uint64_t found = ~0ULL;
+            int fpop = 0;
             bool gave_up = false;
             for (uint64_t probes = 0;; ++probes) {
                 if (probes > st.tmask) { // a full table cannot happen below load 1/2; never spin
@@ -527,6 +539,8 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     for (int w = 0; w < W; ++w) eq = eq && (o[w] == p[w]);
                     if (eq) {
                         found = idx;
+#pragma unroll
+                        for (int w = 0; w < W; ++w) fpop += __popcll(o[w]);
                         break;
                     }
                 }
@@ -550,7 +564,10 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                 const bool follower = (flag & 1) != 0;
                 const bool leader_took_it = follower && ((sc.emit_bits[found >> 5] >> (found & 31)) & 1u);
                 if (!leader_took_it) {
-                    vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
+                    if constexpr (LENK) // pre-gate value: kept by the sweep, or untouched (partner outside the cos set)
+                        vt = fpop <= static_cast<int>(tr.len_k) ? sc.aux[found] : st.coef[found];
+                    else
+                        vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
                     st.coef[src] = __fma_rn(sinv * -ph, vt, st.coef[src]);
                     st.coef[found] = __fma_rn(sinv * ph, v, st.coef[found]);
                     rec = true; // a rotated pair (recorded in replay mode and by a recording forward pass)

@@ -44,13 +44,14 @@ def build(reference_root: str = "/root/reference") -> None:
 class _PortCfg(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower", C.c_int32), ("lower", C.c_double), ("has_upper", C.c_int32),
-                ("upper", C.c_double), ("words", C.c_int32)]
+                ("upper", C.c_double), ("words", C.c_int32), ("has_len_k", C.c_int32), ("len_k", C.c_uint32)]
 
 
 class _RefCfg(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower", C.c_int32), ("lower", C.c_double), ("has_upper", C.c_int32),
-                ("upper", C.c_double), ("partitions", C.c_int32), ("logical_num_modes", C.c_int32)]
+                ("upper", C.c_double), ("partitions", C.c_int32), ("logical_num_modes", C.c_int32),
+                ("len_k", C.c_int32)]
 
 
 _P = np.ctypeslib.ndpointer
@@ -140,9 +141,11 @@ def run_port(wl, params: np.ndarray | None = None, n_layers: int | None = None) 
     lib = _load_port()
     keys, coefs, core = wl.encoded_observable()
     W = wl.words
+    len_k = wl.extra.get("only_rotate_len_k")
     cfg = _PortCfg(_basis_code(wl.basis), _cutoff_code(wl.cutoff_type), wl.cutoff,
                    int(wl.lower_atol is not None), float(wl.lower_atol or 0.0),
-                   int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), W)
+                   int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), W,
+                   int(len_k is not None), int(len_k or 0))
     keys = np.ascontiguousarray(keys, dtype=np.uint64)
     coefs = np.ascontiguousarray(coefs, dtype=np.float64)
     mask = np.ascontiguousarray(wl.state_mask(), dtype=np.uint64)
@@ -191,7 +194,8 @@ class RefEngine:
         st = np.asarray(list(wl.initial_state) or [0], dtype=np.int64)
         cfg = _RefCfg(_basis_code(wl.basis), _cutoff_code(wl.cutoff_type), wl.cutoff,
                       int(wl.lower_atol is not None), float(wl.lower_atol or 0.0),
-                      int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), partitions, wl.num_modes)
+                      int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), partitions, wl.num_modes,
+                      int(wl.extra.get("only_rotate_len_k") or 0))
         err = C.create_string_buffer(1024)
         self._keep = (off, flat, re, im, st)
         self.h = self.lib.mpref_create(C.byref(cfg), len(obs), _ptr(off), _ptr(flat), _ptr(re), _ptr(im),

@@ -13,8 +13,23 @@ from monoprop_b200.workloads import Workload
 GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden")
 
 SEEDED = ["line20", "line20_L200", "hubbard6x6_L400", "ising100_L600", "ising50_d2", "ising50_d3", "ising100_L1200"]
+#: seeded workloads propagated with only_rotate_len_k: name -> (base workload name, layers, k)
+LEN_K = {"line20_k6": ("line20", None, 6), "hubbard6x6_L400_k6": ("hubbard6x6", 400, 6),
+         "ising50_d3_k8": ("ising50_d3", None, 8)}
 REF_CASES = [f"ref_{c}{t}" for c in ("rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact")
              for t in ("", "_atol1e-10")]
+
+
+def len_k_workload(name: str):
+    """(workload with only_rotate_len_k set, layers) of the ``LEN_K`` fixture ``name``."""
+    import dataclasses
+
+    from monoprop_b200 import workloads as W
+
+    base, L, k = LEN_K[name]
+    make = {"line20": W.line20, "hubbard6x6": W.hubbard6x6, "ising50_d3": lambda: W.ising50(3)}[base]
+    wl = make()
+    return dataclasses.replace(wl, extra={**wl.extra, "only_rotate_len_k": k}), L
 
 
 def load(name: str) -> dict:

@@ -18,6 +18,10 @@
  *     append-only inserts in leader-then-follower order (Engine.h:432-444, MPOperator.h:269-278).
  *   - rotation apply with the pre-cos partner value recovered as stored*(1/cos)
  *     (layer_build/FusedApply.h:32-83, Engine.h:209-212,599-614).
+ *   - only_rotate_len_k: a term with more than k set slots takes no part in the gate (neither cos-scaled
+ *     nor emitted; layer_build/Scan.h:146-157,376-391); the gate then runs the two-pass form, partner
+ *     values read unscaled and the cos set (anticommuting terms of at most k slots) scaled before the
+ *     adds (FusedApply.h:46-52, Engine.h:553,599-614).
  *   - <0|O|0> = core + sum over fully paired rows of phase*c (MPOperator.h:235-254,
  *     algebra/PauliAlgebra.h:144-147, algebra/MajoranaAlgebra.h:56-60, MPFunctions.cpp:196-205).
  *
@@ -43,6 +47,8 @@ typedef struct {
     int32_t has_upper;
     double upper;
     int32_t words; /* W, 1..8 */
+    int32_t has_len_k; /* only_rotate_len_k given */
+    uint32_t len_k;
 } mpo_config;
 
 typedef struct {
@@ -277,7 +283,7 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
         const double cosv = cos(2.0 * ang);
         const double sinv = sin(2.0 * ang);
         const double abs_sin = fabs(sinv);
-        const int fused = cosv != 0.0;
+        const int fused = cosv != 0.0 && !s->cfg.has_len_k;
         const double inv_cos = fused ? 1.0 / cosv : 1.0;
         gate_ctx c;
         make_ctx(s, g, &c);
@@ -301,6 +307,7 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
                 if (c.g_odd) par ^= mpop & 1;
                 if (!par) continue;
                 ++n_anti;
+                if (s->cfg.has_len_k && mpop > (int)s->cfg.len_k) continue;
                 const double v = s->coef[i];
                 if (fused) s->coef[i] = v * cosv;
                 const double av = fabs(v);
@@ -353,7 +360,7 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
         if (reserve(s, n0 + n_miss) != 0) return -1;
         c_arr = s->coef;
         if (!fused) {
-            /* two-pass form (cos == 0): every anticommuting term is scaled before the adds */
+            /* two-pass form (cos == 0, or only_rotate_len_k): the cos set is scaled before the adds */
             for (size_t i = 0; i < n0; ++i) {
                 const uint64_t *m = s->keys + i * W;
                 int par = 0, mpop = 0;
@@ -362,7 +369,7 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
                     mpop += popc(m[w]);
                 }
                 if (c.g_odd) par ^= mpop & 1;
-                if (par) c_arr[i] = cosv * c_arr[i];
+                if (par && !(s->cfg.has_len_k && mpop > (int)s->cfg.len_k)) c_arr[i] = cosv * c_arr[i];
             }
         }
         for (size_t k = 0; k < nh; ++k) {

@@ -31,6 +31,7 @@ struct mpref_config {
     double upper;
     int32_t partitions;        // >= 1
     int32_t logical_num_modes; // modes (Majorana) or qubits (Pauli)
+    int32_t len_k;             // only_rotate_len_k, 0 = not given
 };
 }
 
@@ -71,7 +72,9 @@ struct Base {
 template <size_t N>
 struct Impl final : Base {
     std::unique_ptr<MonomialPropagator<N>> p;
+    std::optional<size_t> len_k;
     Impl(const mpref_config &c, const OperatorDict &op, const VecZ &state) {
+        if (c.len_k > 0) len_k = static_cast<size_t>(c.len_k);
         std::optional<double> lo = c.has_lower ? std::optional<double>(c.lower) : std::nullopt;
         std::optional<double> hi = c.has_upper ? std::optional<double>(c.upper) : std::nullopt;
         p = std::make_unique<MonomialPropagator<N>>(op,
@@ -88,10 +91,10 @@ struct Impl final : Base {
                                                     static_cast<size_t>(c.partitions));
     }
     void propagate(const Gates &g, const VecD &params) override {
-        p->propagate(g.monos, g.mapping, g.gen, params, std::nullopt);
+        p->propagate(g.monos, g.mapping, g.gen, params, len_k);
     }
     void build_graph(const Gates &g, const VecD &params) override {
-        p->build_graph(g.monos, g.mapping, g.gen, std::nullopt, params, std::nullopt);
+        p->build_graph(g.monos, g.mapping, g.gen, std::nullopt, params, len_k);
     }
     double ev(const VecD &params) override { return p->expectation_value(params); }
     std::pair<double, VecD> ev_grad(const VecD &params) override { return p->expectation_value_and_gradient(params); }

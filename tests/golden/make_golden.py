@@ -13,18 +13,21 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
   at shifted parameters: expectation and gradient there;
 * ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
   replayed graph;
+* ``<workload>_k<k>.npz`` -- seeded workloads propagated with ``only_rotate_len_k = k``;
 * ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
   (``tests/data/{rx_rz_ry_rz_exact,random_exact,lih_fermionic_spin_exact}.msgpack``), re-expressed as
   engine arrays by this repository's front-end (``Circuit.from_dense_arrays`` + ``expand_monomials``,
   ``MajoranaOperator`` canonicalisation), with the fixture's exact energy and gradient and the reference
   engine's raw output at infinite cutoff (``cutoff = 2 n``).
 
-Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT] [--fd-full]`` (``--fd-full`` adds the slow
-finite-difference golden of the full 100-qubit circuit).
+Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT] [--fd-full] [--len-k-only]`` (``--fd-full``
+adds the slow finite-difference golden of the full 100-qubit circuit; ``--len-k-only`` writes only the
+``only_rotate_len_k`` fixtures).
 """
 
 from __future__ import annotations
 
+import dataclasses
 import hashlib
 import os
 import sys
@@ -51,6 +54,13 @@ SEEDED = [
     ("ising50_d2", lambda: W.ising50(2), None),
     ("ising50_d3", lambda: W.ising50(3), None),
     ("ising100_L1200", W.ising100, 1200),
+]
+
+# only_rotate_len_k cases: (name, workload, layers, k)
+LEN_K = [
+    ("line20_k6", W.line20, None, 6),
+    ("hubbard6x6_L400_k6", W.hubbard6x6, 400, 6),
+    ("ising50_d3_k8", lambda: W.ising50(3), None, 8),
 ]
 
 REF_CASES = ["rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact"]
@@ -109,6 +119,15 @@ def main(reference_root: str = "/root/reference") -> None:
     oracle.build(reference_root)
     if not oracle.ref_available():
         raise SystemExit("reference oracle could not be built")
+    for name, make, L, k in LEN_K:
+        wl = make()
+        wl = dataclasses.replace(wl, extra={**wl.extra, "only_rotate_len_k": k})
+        r = oracle.run_ref(wl, n_layers=L)
+        save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
+                    {"n_layers": np.int64(wl.n_layers if L is None else L), "only_rotate_len_k": np.int64(k)})
+        print(name, r.keys.shape[0], r.expectation)
+    if "--len-k-only" in sys.argv:
+        return
     for name, make, L in SEEDED:
         wl = make()
         r = oracle.run_ref(wl, n_layers=L)

@@ -6,8 +6,11 @@
 * against the reference engine itself, live, when oracle/_ref/libmpref.so has been built here
   (random Pauli and Majorana circuits exercising lower_atol, upper_atol rescue, odd-weight generators,
   near-zero cosines and the fully-paired exemption);
-* on the analytic one-gate truncation cases of the reference's tests/test_coeff_trunc.py:59-96.
+* on the analytic one-gate truncation cases of the reference's tests/test_coeff_trunc.py:59-96;
+* with only_rotate_len_k, against its golden fixtures and the live reference.
 """
+
+import dataclasses
 
 import numpy as np
 import pytest
@@ -46,6 +49,28 @@ def test_port_reproduces_reference_fixture(name):
 @pytest.mark.parametrize("basis", ["pauli", "majorana"])
 def test_port_matches_reference_live(seed, basis):
     wl = random_workload(seed, basis)
+    a, b = oracle.run_port(wl), oracle.run_ref(wl)
+    ia, ib = canonical_order(a.keys), canonical_order(b.keys)
+    assert np.array_equal(a.keys[ia], b.keys[ib])
+    assert np.array_equal(a.coefs[ia], b.coefs[ib])
+    assert a.expectation == b.expectation
+
+
+@pytest.mark.parametrize("name", sorted(golden.LEN_K))
+def test_port_matches_reference_golden_len_k(name):
+    """only_rotate_len_k (Scan.h:146-157,376-391): terms longer than k sit out the gate."""
+    wl, L = golden.len_k_workload(name)
+    r = oracle.run_port(wl, n_layers=L)
+    golden.check_against(golden.load(name), r.keys, r.coefs, r.expectation)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built here")
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("basis", ["pauli", "majorana"])
+@pytest.mark.parametrize("k", [2, 4, 6])
+def test_port_matches_reference_live_len_k(seed, basis, k):
+    base = random_workload(seed, basis)
+    wl = dataclasses.replace(base, extra={**base.extra, "only_rotate_len_k": k})
     a, b = oracle.run_port(wl), oracle.run_ref(wl)
     ia, ib = canonical_order(a.keys), canonical_order(b.keys)
     assert np.array_equal(a.keys[ia], b.keys[ib])
