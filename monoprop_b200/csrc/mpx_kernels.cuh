@@ -84,8 +84,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     __shared__ uint32_t s_qn;               // the block's queries so far
     __shared__ uint32_t s_red[kWarps];
     __shared__ uint32_t s_fold[kMaxFoldCols];
-    if (cnt->stall != kNoStall) return;
+    // the counters and the gate's fold columns are read together (one memory latency, not two)
+    const GateDesc &gd = gates[gate];
+    const uint32_t stall = cnt->stall;
     const uint64_t n0 = cnt->n;
+    const int n_fold = gd.n_fold;
+    const uint32_t fcol = threadIdx.x < kMaxFoldCols ? gd.fold_cols[threadIdx.x] : 0u;
+    const bool empty = gd.empty != 0, g_odd = gd.g_odd != 0;
+    const uint32_t pivot_col = gd.pivot_col;
+    if (stall != kNoStall) return;
     if (2 * n0 > st.cap) {
         // Not enough room for the worst case (every term appends its partner): stop here, untouched,
         // and let the host grow the store and re-issue this step.
@@ -99,10 +106,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
             if (tp.r_begin != nullptr) tp.r_begin[step] = cnt->rec_total;
         }
     }
-    const GateDesc &gd = gates[gate];
-    const int n_fold = gd.n_fold;
     const SweepGeometry geo = sweep_geometry(n0);
-    if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = threadIdx.x < n_fold ? gd.fold_cols[threadIdx.x] : 0;
+    if (threadIdx.x < kMaxFoldCols) s_fold[threadIdx.x] = static_cast<int>(threadIdx.x) < n_fold ? fcol : 0;
     if (threadIdx.x == 0) s_qn = 0;
     if constexpr (REPLAY) {
         if (threadIdx.x < kWarps)
@@ -113,11 +118,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t anti_count = 0;
-    if (!gd.empty && n0 != 0) {
+    if (!empty && n0 != 0) {
         const double cosv = gd.cosv, sinabs = gd.abs_sin;
         const bool cos_zero = gd.cos_zero != 0;
         const int gpop = gd.gpop;
-        const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(gd.pivot_col) * st.cstride;
+        const uint32_t *__restrict__ pivot = st.cols + static_cast<uint64_t>(pivot_col) * st.cstride;
         const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
         const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
         const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                             }
                         }
                     }
-                    if (gd.g_odd) anti ^= parity[j];
+                    if (g_odd) anti ^= parity[j];
                     if (j == geo.nwords - 1) anti &= tail;
                     foll = anti & pivot[j];
                 }
@@ -479,14 +484,17 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                                                      Trunc tr, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
     __shared__ unsigned long long s_base, s_rbase;
-    if (cnt->stall != kNoStall) return;
-    const uint64_t n0 = cnt->n0;
+    // counters, this block's query count and the gate are read together (one memory latency)
     const GateDesc &gd = gates[gate];
+    const uint32_t stall = cnt->stall;
+    const uint64_t n0 = cnt->n0;
+    const uint32_t total = sc.blk_q[blockIdx.x];
+    const bool empty = gd.empty != 0;
+    if (stall != kNoStall) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const SweepGeometry geo = sweep_geometry(n0);
-    if (gd.empty || n0 == 0) return;
-    const uint32_t total = sc.blk_q[blockIdx.x];
+    if (empty || n0 == 0) return;
     if (total == 0) return;
     const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
     uint64_t g[W];
