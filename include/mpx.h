@@ -125,6 +125,13 @@ MPX_API mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double v
  * reference's message. The gradient and graph entry points reject an engine with k set. */
 MPX_API mpx_status mpx_set_only_rotate_len_k(mpx_engine *e, int64_t k);
 
+/* basis_change of a Majorana engine (the constructor argument, MonomialPropagator.inl:82-131,460-495):
+ * rows[s] (W words, encoded like a key) is the monomial slot s maps to; n_rows must be 2*num_modes. The
+ * structural cutoff of every emitted partner P is then judged on XOR_{s in P} rows[s] (change_basis,
+ * MajoranaAlgebra.h:179-189), the Jordan-Wigner image cutoff. n_rows = 0 clears it. Pauli engines reject
+ * it with the reference's message. */
+MPX_API mpx_status mpx_set_basis_change(mpx_engine *e, const uint64_t *rows, uint32_t n_rows);
+
 /* Device pointers of the live store (keys [n][W], coefficients [n]) for in-process consumers such as
  * the torch wrapper; valid until the next mutating call. */
 MPX_API mpx_status mpx_device_view(mpx_engine *e, const uint64_t **keys, double **coefs, uint64_t *n);

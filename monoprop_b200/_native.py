@@ -22,7 +22,7 @@ _STATUS = {1: "MPX_ERR_INVALID", 2: "MPX_ERR_CUDA", 3: "MPX_ERR_NOMEM", 4: "MPX_
 EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_set_angles", "mpx_propagate_circuit",
             "mpx_circuit_destroy", "mpx_expectation", "mpx_size", "mpx_words", "mpx_export", "mpx_gate_stats",
             "mpx_reset", "mpx_set_cutoff", "mpx_set_lower_atol", "mpx_set_upper_atol",
-            "mpx_set_only_rotate_len_k", "mpx_device_view",
+            "mpx_set_only_rotate_len_k", "mpx_set_basis_change", "mpx_device_view",
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_graph_build", "mpx_graph_expectation",
             "mpx_graph_gradient", "mpx_set_pair_log", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
@@ -77,6 +77,7 @@ def load() -> C.CDLL:
             "mpx_set_lower_atol": (st, [vp, C.c_int32, C.c_double]),
             "mpx_set_upper_atol": (st, [vp, C.c_int32, C.c_double]),
             "mpx_set_only_rotate_len_k": (st, [vp, C.c_int64]),
+            "mpx_set_basis_change": (st, [vp, vp, C.c_uint32]),
             "mpx_device_view": (st, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u64)]),
             "mpx_stream": (st, [vp, C.POINTER(vp)]),
             "mpx_launch_count": (st, [vp, C.POINTER(u64)]),
@@ -167,6 +168,7 @@ class Engine:
                      float(upper_atol or 0.0), int(num_modes), int(device), int(capacity_hint),
                      int(blocks_per_sm), int(table_shift))
         self.words = (int(num_modes) + 31) // 32
+        self.num_modes = int(num_modes)
         k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, self.words)
         c = np.ascontiguousarray(coefs, dtype=np.float64).reshape(-1)
         m = np.ascontiguousarray(state_mask, dtype=np.uint64).reshape(-1)
@@ -242,6 +244,16 @@ class Engine:
         """only_rotate_len_k of the next propagate calls (None clears it)."""
         self._check(self.lib.mpx_set_only_rotate_len_k(self.h, 0 if k is None else int(k)))
 
+    def set_basis_change(self, basis_change) -> None:
+        """basis_change rows (one slot list per slot, 2 * num_modes of them), or None to clear."""
+        if basis_change is None:
+            self._check(self.lib.mpx_set_basis_change(self.h, None, 0))
+            return
+        from .encoding import basis_rows
+
+        rows = np.ascontiguousarray(basis_rows(basis_change, self.num_modes)[: 2 * self.num_modes])
+        self._check(self.lib.mpx_set_basis_change(self.h, _p(rows), rows.shape[0]))
+
     def stream(self) -> int:
         s = C.c_void_p()
         self._check(self.lib.mpx_stream(self.h, C.byref(s)))
@@ -311,6 +323,13 @@ class Engine:
 def engine_for(wl, **kw) -> Engine:
     """Engine holding workload ``wl``'s observable (see :mod:`monoprop_b200.workloads`)."""
     keys, coefs, core = wl.encoded_observable()
-    return Engine(basis=wl.basis, cutoff_type=wl.cutoff_type, cutoff=wl.cutoff, num_modes=wl.num_modes,
-                  keys=keys, coefs=coefs, core=core, state_mask=wl.state_mask(), lower_atol=wl.lower_atol,
-                  upper_atol=wl.upper_atol, **kw)
+    eng = Engine(basis=wl.basis, cutoff_type=wl.cutoff_type, cutoff=wl.cutoff, num_modes=wl.num_modes,
+                 keys=keys, coefs=coefs, core=core, state_mask=wl.state_mask(), lower_atol=wl.lower_atol,
+                 upper_atol=wl.upper_atol, **kw)
+    if wl.extra.get("basis_change") is not None:  # a constructor argument of the reference propagator
+        try:
+            eng.set_basis_change(wl.extra["basis_change"])
+        except Exception:
+            eng.close()
+            raise
+    return eng

@@ -7,9 +7,9 @@
 // export of evolved_operator (MonomialPropagator.inl:1099-1127).
 //
 // Scope: the Heisenberg picture -- propagate, and build_graph + expectation_value[_and_gradient](parameters)
-// over the engine's frozen structure (mpx_graph_*). schrodinger_cutoff, basis_change, only_rotate_len_k in
-// build_graph, graph functionals with paring, contract_partially and MPI communicators raise
-// NotImplementedError.
+// over the engine's frozen structure (mpx_graph_*), with basis_change (Majorana) and, for propagate,
+// only_rotate_len_k. schrodinger_cutoff, only_rotate_len_k in build_graph, graph functionals with paring,
+// contract_partially and MPI communicators raise NotImplementedError.
 #include <pybind11/complex.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -93,10 +93,15 @@ public:
         if (cfg_.basis == MPX_BASIS_PAULI && cfg_.cutoff_type != MPX_CUTOFF_SUPPORT)
             throw CutoffConfigError("Pauli basis requires cutoff_type == Support (Length has no Pauli-weight meaning "
                                     "under the Pauli encoding).");
+        // validate_cutoff_config_ (MonomialPropagator.inl:460-481)
         if (basis_change.has_value()) {
             if (cfg_.basis == MPX_BASIS_PAULI)
-                throw CutoffConfigError("Pauli basis does not support basis_change.");
-            throw NotSupported("basis_change: not implemented by the B200 engine");
+                throw CutoffConfigError("Pauli basis does not accept a basis_change (the encoding is already the "
+                                        "Jordan-Wigner image).");
+            if (basis_change->size() != 2 * logical_)
+                throw CutoffConfigError("basis_change must have exactly 2*logical_num_modes (" +
+                                        std::to_string(2 * logical_) + ") rows; got " +
+                                        std::to_string(basis_change->size()) + ".");
         }
         if (upper_atol && lower_atol && *upper_atol < *lower_atol)
             throw PropagatorConfigError("upper_atol (" + std::to_string(*upper_atol) +
@@ -135,9 +140,56 @@ public:
             occ.push_back(2 * m);
         }
         encode(occ, 2 * Tier, mask.data());
+        const std::vector<uint64_t> rows = basis_rows(basis_change);
         check(mpx_create(&cfg_, keys.empty() ? nullptr : keys.data(), coefs.empty() ? nullptr : coefs.data(),
                          coefs.size(), core_, mask.data(), &e_),
               nullptr);
+        if (!rows.empty()) {
+            const mpx_status st = mpx_set_basis_change(e_, rows.data(), static_cast<uint32_t>(2 * Tier));
+            if (st != MPX_OK) {
+                const std::string msg = mpx_last_error(e_);
+                mpx_destroy(e_);
+                e_ = nullptr;
+                throw std::runtime_error(msg);
+            }
+            basis_change_ = basis_change;
+        }
+    }
+
+    // basis_change rows by slot, each slot set once (indices_to_bitset_checked, AlgebraCommon.h:44-63); the
+    // rows of the slots above 2 * logical_num_modes stay zero. Empty when there is no basis change.
+    std::vector<uint64_t> basis_rows(const std::optional<std::vector<std::vector<size_t>>> &basis_change) const {
+        std::vector<uint64_t> rows;
+        if (!basis_change.has_value()) return rows;
+        rows.assign(2 * Tier * kWords, 0);
+        for (size_t r = 0; r < basis_change->size(); ++r)
+            for (size_t s : (*basis_change)[r]) {
+                if (s >= 2 * logical_)
+                    throw std::runtime_error("Majorana/Pauli index " + std::to_string(s) +
+                                             " is out of range; must be less than " + std::to_string(2 * logical_) + ".");
+                const size_t b = 2 * Tier - 1 - s;
+                rows[r * kWords + b / 64] |= 1ULL << (b % 64);
+            }
+        return rows;
+    }
+
+    // basis_change property (binder.h:185-188; update_basis_change validates like the constructor)
+    std::optional<std::vector<std::vector<size_t>>> basis_change() const { return basis_change_; }
+    void set_basis_change(const std::optional<std::vector<std::vector<size_t>>> &basis_change) {
+        if (basis_change.has_value()) {
+            if (cfg_.basis == MPX_BASIS_PAULI)
+                throw CutoffConfigError("Pauli basis does not accept a basis_change (the encoding is already the "
+                                        "Jordan-Wigner image).");
+            if (basis_change->size() != 2 * logical_)
+                throw CutoffConfigError("basis_change must have exactly 2*logical_num_modes (" +
+                                        std::to_string(2 * logical_) + ") rows; got " +
+                                        std::to_string(basis_change->size()) + ".");
+        }
+        const std::vector<uint64_t> rows = basis_rows(basis_change);
+        check(mpx_set_basis_change(e_, rows.empty() ? nullptr : rows.data(),
+                                   rows.empty() ? 0u : static_cast<uint32_t>(2 * Tier)),
+              e_);
+        basis_change_ = basis_change;
     }
 
     ~Propagator() {
@@ -361,6 +413,7 @@ private:
     }
 
     mpx_config cfg_{};
+    std::optional<std::vector<std::vector<size_t>>> basis_change_;
     size_t logical_;
     std::vector<size_t> state_;
     double core_ = 0.0;
@@ -404,6 +457,7 @@ void bind(py::module_ &m) {
         .def_property("lower_atol", &P::lower_atol, &P::set_lower_atol)
         .def_property("upper_atol", &P::upper_atol, &P::set_upper_atol)
         .def_property_readonly("cutoff_type", &P::cutoff_type)
+        .def_property("basis_change", &P::basis_change, &P::set_basis_change)
         .def_property_readonly("basis", &P::basis)
         .def_property_readonly("num_modes", &P::num_modes)
         .def_property_readonly("schrodinger", [](P &) { return false; })

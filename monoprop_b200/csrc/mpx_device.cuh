@@ -41,6 +41,8 @@ struct Trunc {
     // only_rotate_len_k: terms with more than len_k set slots take no part in a gate (Scan.h:146-157)
     int32_t has_len_k;
     uint32_t len_k;
+    // basis_change (Majorana): [2T][W] device rows by slot; the partner's cutoff is judged on its image
+    const uint64_t *basis_rows;
 };
 
 // Device counters, one set per engine.
@@ -164,6 +166,35 @@ __device__ __forceinline__ bool keep_partner(const uint64_t (&p)[W], int ppop, c
     if (xs == 0) return true; // fully paired terms are always kept
     const int measure = tr.cutoff_type == 1 ? os : ppop;
     return measure <= static_cast<int>(tr.cutoff);
+}
+
+// Structural keep test under basis_change (MonomialPropagatorCommon.h:44-62, change_basis
+// MajoranaAlgebra.h:179-189): the image XOR_{slot s in P} row_s is judged by the cutoff, with no popcount
+// shortcut (the reference's evaluator falls through to the stored function, AlgebraCommon.h:229-243).
+template <int W>
+__device__ __forceinline__ bool keep_partner_mapped(const uint64_t (&p)[W], const Trunc &tr) {
+    uint64_t q[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) q[w] = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        for (uint64_t x = p[w]; x != 0; x &= x - 1) {
+            const int slot = 64 * W - 1 - (64 * w + __ffsll(static_cast<long long>(x)) - 1);
+            const uint64_t *row = tr.basis_rows + static_cast<uint64_t>(slot) * W;
+#pragma unroll
+            for (int v = 0; v < W; ++v) q[v] ^= __ldg(row + v);
+        }
+    }
+    int xs = 0, os = 0, pop = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        const uint64_t a = q[w] & kEven, b = (q[w] >> 1) & kEven;
+        xs += __popcll(a ^ b);
+        os += __popcll(a | b);
+        pop += __popcll(q[w]);
+    }
+    if (xs == 0) return true;
+    return (tr.cutoff_type == 1 ? os : pop) <= static_cast<int>(tr.cutoff);
 }
 
 // Rotation phase of the sine branch M -> M^G.

@@ -128,7 +128,12 @@ struct mpx_engine {
     std::vector<GraphEntry> graphs;
     uint64_t store_gen = 0;
     uint64_t rec_hint = 0;
-    int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity // pair records the last recording forward pass needed (sizes the next log)
+    int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity
+    uint64_t *d_basis = nullptr; // basis_change rows [2T][W] (tr.basis_rows points here when set)
+    // Large blocks through the kept-block cache (dev_alloc). The batch runner turns it off for its
+    // engines: with several engines growing at once, power-of-two classes and idle kept blocks crowd
+    // the device, and a 96-instance gradient batch took 2x longer with them.
+    bool keep_blocks = true; // pair records the last recording forward pass needed (sizes the next log)
     bool use_graphs = true;
     bool small_path = true; // run small stores in one shared-memory block (mpx_small.cuh)
     std::string err;
@@ -142,7 +147,10 @@ std::atomic<uint64_t> g_circuit_ids{1};
     do {                                                                                                            \
         cudaError_t e_ = (call);                                                                                    \
         if (e_ != cudaSuccess) {                                                                                    \
-            return fail(eng, MPX_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));                      \
+            /* out of memory is MPX_ERR_NOMEM (callers may retry once memory is released) */                      \
+            if (e_ == cudaErrorMemoryAllocation) cudaGetLastError();                                              \
+            return fail(eng, e_ == cudaErrorMemoryAllocation ? MPX_ERR_NOMEM : MPX_ERR_CUDA,                       \
+                        std::string(#call ": ") + cudaGetErrorString(e_));                                          \
         }                                                                                                           \
     } while (0)
 
@@ -232,7 +240,7 @@ void release_kept_blocks(int device) {
 
 cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
     BlockCache &c = block_cache();
-    if (bytes < kKeepMin) {
+    if (bytes < kKeepMin || !e->keep_blocks) {
         const cudaError_t ce = cudaMallocFromPoolAsync(ptr, bytes, e->pool, e->stream);
         if (ce == cudaSuccess) { // an address is never on record as a kept class while it is a small block
             std::lock_guard<std::mutex> lock(c.mu);
@@ -298,31 +306,52 @@ void dev_free(mpx_engine *e, void *ptr) { dev_release(e->device, e->stream, ptr)
 
 // ----- kernel dispatch over (W, basis) ------------------------------------------------------------------
 
-template <int W, int B>
-void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
-    cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
+template <int W, int B, int EXT>
+void launch_gate_ext(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], e->stream);
-    if (e->tr.has_len_k)
-        k_sweep<W, B, false, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
-                                                                      e->fwd_tape, e->d_stats);
-    else
-        k_sweep<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
-                                                         e->fwd_tape, e->d_stats);
+    k_sweep<W, B, false, EXT><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
+                                                                 e->fwd_tape, e->d_stats);
     if (ev) cudaEventRecord(ev[1], e->stream);
-    if (e->tr.has_len_k)
-        k_resolve<W, B, false, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step,
-                                                                        e->tr, e->fwd_tape);
-    else
-        k_resolve<W, B><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
-                                                           e->fwd_tape);
+    k_resolve<W, B, false, (EXT & 1) != 0><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate,
+                                                                               step, e->tr, e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
 }
 
-// A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends.
+// One gate: the sweep/resolve variant of the engine's options (only_rotate_len_k; basis_change, which only
+// Majorana engines accept).
+template <int W, int B>
+void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step) {
+    cudaEvent_t *ev = e->profile ? &e->pev[4 * static_cast<size_t>(step)] : nullptr;
+    const int ext = (e->tr.has_len_k ? 1 : 0) | (e->tr.basis_rows != nullptr ? 2 : 0);
+    if constexpr (B == 0) {
+        switch (ext) {
+        case 0: launch_gate_ext<W, B, 0>(e, d_desc, gate, step, ev); break;
+        case 1: launch_gate_ext<W, B, 1>(e, d_desc, gate, step, ev); break;
+        case 2: launch_gate_ext<W, B, 2>(e, d_desc, gate, step, ev); break;
+        default: launch_gate_ext<W, B, 3>(e, d_desc, gate, step, ev); break;
+        }
+    }
+    else {
+        if (ext & 1) launch_gate_ext<W, B, 1>(e, d_desc, gate, step, ev);
+        else launch_gate_ext<W, B, 0>(e, d_desc, gate, step, ev);
+    }
+}
+
+// A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends. (The
+// gradient rejects only_rotate_len_k; basis_change changes only the emit decisions, replayed alike.)
 template <int W, int B>
 void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
-    k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp,
-                                                           e->d_stats);
+    bool mapped = false;
+    if constexpr (B == 0) {
+        if (e->tr.basis_rows != nullptr) {
+            k_sweep<W, B, true, 2><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step,
+                                                                      e->tr, tp, e->d_stats);
+            mapped = true;
+        }
+    }
+    if (!mapped)
+        k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp,
+                                                               e->d_stats);
     k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
     k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
 }
@@ -736,7 +765,8 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     uint64_t pending_slot = 0;
     // Small store: run gates in one shared-memory block until the store outgrows it (or the range ends).
     bool used_small = false;
-    if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && !e->tr.has_len_k && e->fwd_tape.w_anti == nullptr &&
+    if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && !e->tr.has_len_k && e->tr.basis_rows == nullptr &&
+        e->fwd_tape.w_anti == nullptr &&
         hi - lo >= 8) {
         MPX_CUDA(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
         MPX_CUDA(cudaStreamSynchronize(e->stream));
@@ -1075,7 +1105,9 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         cudaError_t e2_ = (call);                                                                                   \
         if (e2_ != cudaSuccess) {                                                                                   \
             release();                                                                                              \
-            return fail(eng, MPX_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e2_));                     \
+            if (e2_ == cudaErrorMemoryAllocation) cudaGetLastError();                                             \
+            return fail(eng, e2_ == cudaErrorMemoryAllocation ? MPX_ERR_NOMEM : MPX_ERR_CUDA,                      \
+                        std::string(#call ": ") + cudaGetErrorString(e2_));                                         \
         }                                                                                                           \
     } while (0)
     MPX_CUDA_REL(cudaMemcpyAsync(d_steps, u_base.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
@@ -1668,6 +1700,34 @@ mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value) {
     return MPX_OK;
 }
 
+mpx_status mpx_set_basis_change(mpx_engine *e, const uint64_t *rows, uint32_t n_rows) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    mpx_engine *eng = e;
+    if (n_rows == 0) {
+        clear_graphs(e);
+        e->tr.basis_rows = nullptr;
+        return MPX_OK;
+    }
+    if (e->cfg.basis != 0)
+        return fail(e, MPX_ERR_INVALID,
+                    "Pauli basis does not accept a basis_change (the encoding is already the Jordan-Wigner image).");
+    if (n_rows != 2 * static_cast<uint32_t>(e->cfg.num_modes))
+        return fail(e, MPX_ERR_INVALID, "basis_change must have exactly 2*logical_num_modes (" +
+                                            std::to_string(2 * e->cfg.num_modes) + ") rows; got " +
+                                            std::to_string(n_rows) + ".");
+    if (rows == nullptr) return fail(e, MPX_ERR_INVALID, "basis_change rows are NULL");
+    MPX_CUDA(cudaSetDevice(e->device));
+    const size_t bytes = static_cast<size_t>(64 * e->W) * e->W * sizeof(uint64_t); // 2T rows of W words
+    if (e->d_basis == nullptr) MPX_CUDA(cudaMalloc(reinterpret_cast<void **>(&e->d_basis), bytes));
+    MPX_CUDA(cudaMemsetAsync(e->d_basis, 0, bytes, e->stream));
+    MPX_CUDA(cudaMemcpyAsync(e->d_basis, rows, static_cast<size_t>(n_rows) * e->W * sizeof(uint64_t),
+                             cudaMemcpyHostToDevice, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    clear_graphs(e);
+    e->tr.basis_rows = e->d_basis;
+    return MPX_OK;
+}
+
 mpx_status mpx_set_only_rotate_len_k(mpx_engine *e, int64_t k) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     const int64_t max_k = 2 * static_cast<int64_t>(e->cfg.num_modes);
@@ -1819,6 +1879,11 @@ mpx_status mpx_trim_device_memory(int32_t device) {
     return MPX_OK;
 }
 
+// Internal (not exported): the batch runner's engines allocate straight from the pool.
+void mpx_internal_block_keeping(mpx_engine *e, int32_t on) {
+    if (e != nullptr) e->keep_blocks = on != 0;
+}
+
 const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }
 
 void mpx_destroy(mpx_engine *e) {
@@ -1844,6 +1909,7 @@ void mpx_destroy(mpx_engine *e) {
     cudaFreeHost(e->h_out);
     cudaFree(e->d_init_keys);
     cudaFree(e->d_init_coef);
+    cudaFree(e->d_basis);
     dev_free(e, e->d_stats);
     if (e->stream != nullptr) {
         cudaStreamSynchronize(e->stream); // the pool frees above are stream-ordered

@@ -69,7 +69,8 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 // query region (one shared-counter bump per warp and round). With a tape, each warp's anticommuting
 // count is saved per step (forward pass of a gradient) and, in REPLAY mode, every anticommuting term's
 // index and pre-gate coefficient go to the undo log at its chunk-owning warp's precomputed offset.
-template <int W, int BASIS, bool REPLAY = false, bool LENK = false>
+// EXT: bit 0 only_rotate_len_k, bit 1 basis_change (instantiated only where the engine uses them).
+template <int W, int BASIS, bool REPLAY = false, int EXT = 0>
 __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                    Trunc tr, Tape tp, uint64_t *__restrict__ stats) {
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                     bool emit = false, follower = false;
                     int phase = 0;
                     bool member = L >= 0;
-                    if (LENK && member) {
+                    if ((EXT & 1) && member) {
                         // only_rotate_len_k: a term of more than len_k slots is left alone by this gate
                         // (no cos scaling, no emit); the partner values of the others are kept in `aux`
                         uint64_t mk[W];
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                     if (member) {
                         follower = (s_foll[ow][word] >> (l & 31)) & 1u;
                         st.coef[term] = v * cosv;
-                        if (cos_zero || LENK) sc.aux[term] = v;
+                        if (cos_zero || (EXT & 1)) sc.aux[term] = v;
                         if constexpr (REPLAY) {
                             const uint64_t rr = s_ubase[ow] + static_cast<uint64_t>(k + kBlock * r +
                                                                                      static_cast<int>(threadIdx.x) -
@@ -273,7 +274,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
                                 ov += __popcll(m[w] & gw);
                             }
                             const int ppop = mpop + gpop - 2 * ov;
-                            if (keep_partner<W>(p, ppop, tr) || (tr.has_upper && sinabs * av >= tr.upper)) {
+                            bool keep;
+                            if constexpr ((EXT & 2) != 0) keep = keep_partner_mapped<W>(p, tr);
+                            else keep = keep_partner<W>(p, ppop, tr);
+                            if (keep || (tr.has_upper && sinabs * av >= tr.upper)) {
                                 emit = true;
                                 phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
                             }

@@ -54,6 +54,19 @@ def encode_many(monomials: Sequence[Sequence[int]], num_modes: int) -> np.ndarra
     return out
 
 
+def basis_rows(basis_change: Sequence[Sequence[int]], num_modes: int) -> np.ndarray:
+    """``uint64[2T, W]``: row s is the monomial slot s maps to under ``basis_change`` (its listed slots set,
+    as ``indices_to_bitset_checked``, ``AlgebraCommon.h:44-63``); rows of slots >= 2 * num_modes are zero."""
+    if len(basis_change) != 2 * num_modes:
+        raise ValueError(f"basis_change must have exactly 2*logical_num_modes ({2 * num_modes}) rows; "
+                         f"got {len(basis_change)}.")
+    tier = storage_tier(num_modes)
+    out = np.zeros((2 * tier, tier // 32), dtype=np.uint64)
+    for s, row in enumerate(basis_change):
+        out[s] = slots_to_words(sorted(set(int(x) for x in row)), num_modes)
+    return out
+
+
 def words_to_slots(words: np.ndarray, num_modes: int) -> tuple[int, ...]:
     """Decode one key (``uint64[W]``) into its ascending slot tuple."""
     tier = storage_tier(num_modes)

@@ -44,7 +44,8 @@ def build(reference_root: str = "/root/reference") -> None:
 class _PortCfg(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower", C.c_int32), ("lower", C.c_double), ("has_upper", C.c_int32),
-                ("upper", C.c_double), ("words", C.c_int32), ("has_len_k", C.c_int32), ("len_k", C.c_uint32)]
+                ("upper", C.c_double), ("words", C.c_int32), ("has_len_k", C.c_int32), ("len_k", C.c_uint32),
+                ("basis_rows", C.c_void_p)]
 
 
 class _RefCfg(C.Structure):
@@ -104,7 +105,8 @@ def _load_ref() -> C.CDLL:
         lib = C.CDLL(REF_LIB)
         lib.mpref_create.restype = C.c_void_p
         lib.mpref_create.argtypes = [C.POINTER(_RefCfg), C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                     C.c_size_t, C.c_void_p, C.c_char_p, C.c_size_t]
+                                     C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p,
+                                     C.c_size_t]
         lib.mpref_propagate.restype = C.c_int
         lib.mpref_propagate.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_size_t, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_char_p,
@@ -142,10 +144,15 @@ def run_port(wl, params: np.ndarray | None = None, n_layers: int | None = None) 
     keys, coefs, core = wl.encoded_observable()
     W = wl.words
     len_k = wl.extra.get("only_rotate_len_k")
+    rows = None
+    if wl.extra.get("basis_change") is not None:
+        from monoprop_b200.encoding import basis_rows
+
+        rows = np.ascontiguousarray(basis_rows(wl.extra["basis_change"], wl.num_modes))
     cfg = _PortCfg(_basis_code(wl.basis), _cutoff_code(wl.cutoff_type), wl.cutoff,
                    int(wl.lower_atol is not None), float(wl.lower_atol or 0.0),
                    int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), W,
-                   int(len_k is not None), int(len_k or 0))
+                   int(len_k is not None), int(len_k or 0), None if rows is None else rows.ctypes.data)
     keys = np.ascontiguousarray(keys, dtype=np.uint64)
     coefs = np.ascontiguousarray(coefs, dtype=np.float64)
     mask = np.ascontiguousarray(wl.state_mask(), dtype=np.uint64)
@@ -198,8 +205,12 @@ class RefEngine:
                       int(wl.extra.get("only_rotate_len_k") or 0))
         err = C.create_string_buffer(1024)
         self._keep = (off, flat, re, im, st)
+        bc = wl.extra.get("basis_change")
+        boff, bflat = _flat_slots(bc) if bc is not None else (np.zeros(1, np.int64), np.zeros(1, np.int64))
+        self._keep = (off, flat, re, im, st, boff, bflat)
         self.h = self.lib.mpref_create(C.byref(cfg), len(obs), _ptr(off), _ptr(flat), _ptr(re), _ptr(im),
-                                       len(wl.initial_state), _ptr(st), err, 1024)
+                                       len(wl.initial_state), _ptr(st), 0 if bc is None else len(bc), _ptr(boff),
+                                       _ptr(bflat), err, 1024)
         if not self.h:
             raise RuntimeError(err.value.decode())
 

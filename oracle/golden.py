@@ -14,10 +14,39 @@ GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 SEEDED = ["line20", "line20_L200", "hubbard6x6_L400", "ising100_L600", "ising50_d2", "ising50_d3", "ising100_L1200"]
 #: seeded workloads propagated with only_rotate_len_k: name -> (base workload name, layers, k)
-LEN_K = {"line20_k6": ("line20", None, 6), "hubbard6x6_L400_k6": ("hubbard6x6", 400, 6),
+LEN_K = {"line20_k6": ("line20", None, 6), "hubbard6x6_L400_k4": ("hubbard6x6", 400, 4),
          "ising50_d3_k8": ("ising50_d3", None, 8)}
 REF_CASES = [f"ref_{c}{t}" for c in ("rx_rz_ry_rz_exact", "random_exact", "lih_fermionic_spin_exact")
              for t in ("", "_atol1e-10")]
+
+
+#: seeded Majorana workloads with a basis_change: name -> (base workload name, layers, basis pattern)
+BASIS_CHANGE = {"hubbard6x6_L400_bcjw": ("hubbard6x6", 400, "jw"),
+                "hubbard6x6_L400_bcrand": ("hubbard6x6", 400, "rand")}
+
+
+def basis_pattern(kind: str, num_modes: int, seed: int = 7) -> list[list[int]]:
+    """basis_change rows: "jw" maps slot 2q to {2q} and 2q+1 to {2q, 2q+1}; "perm" is a seeded slot
+    permutation; "rand" gives each slot a seeded random monomial of 1 to 3 slots."""
+    rng = np.random.default_rng(seed)
+    if kind == "jw":
+        return [[s] if s % 2 == 0 else [s - 1, s] for s in range(2 * num_modes)]
+    if kind == "perm":
+        p = rng.permutation(2 * num_modes)
+        return [[int(p[s])] for s in range(2 * num_modes)]
+    return [sorted(set(int(x) for x in rng.choice(2 * num_modes, size=int(rng.integers(1, 4)), replace=False)))
+            for _ in range(2 * num_modes)]
+
+
+def basis_change_workload(name: str):
+    """(workload with basis_change set, layers) of the ``BASIS_CHANGE`` fixture ``name``."""
+    import dataclasses
+
+    from monoprop_b200 import workloads as W
+
+    base, L, kind = BASIS_CHANGE[name]
+    wl = {"hubbard6x6": W.hubbard6x6}[base]()
+    return dataclasses.replace(wl, extra={**wl.extra, "basis_change": basis_pattern(kind, wl.num_modes)}), L
 
 
 def len_k_workload(name: str):

@@ -22,6 +22,8 @@
  *     nor emitted; layer_build/Scan.h:146-157,376-391); the gate then runs the two-pass form, partner
  *     values read unscaled and the cos set (anticommuting terms of at most k slots) scaled before the
  *     adds (FusedApply.h:46-52, Engine.h:553,599-614).
+ *   - basis_change: the structural cutoff of a partner is judged on its image under the given basis rows
+ *     (algebra/MajoranaAlgebra.h:179-189, detail/monomial_propagator/MonomialPropagatorCommon.h:44-62).
  *   - <0|O|0> = core + sum over fully paired rows of phase*c (MPOperator.h:235-254,
  *     algebra/PauliAlgebra.h:144-147, algebra/MajoranaAlgebra.h:56-60, MPFunctions.cpp:196-205).
  *
@@ -49,6 +51,8 @@ typedef struct {
     int32_t words; /* W, 1..8 */
     int32_t has_len_k; /* only_rotate_len_k given */
     uint32_t len_k;
+    /* basis_change: [2T][W] rows indexed by slot (rows of slots >= 2 * logical modes are zero), or NULL */
+    const uint64_t *basis_rows;
 } mpo_config;
 
 typedef struct {
@@ -152,8 +156,26 @@ static void interleave_mask(const uint64_t *g, uint64_t *out, int W) {
     }
 }
 
-static int keep_struct(const mpo_state *s, const uint64_t *p, int pop) {
+static int keep_struct(const mpo_state *s, const uint64_t *p_in, int pop) {
     const int W = s->cfg.words;
+    const uint64_t *p = p_in;
+    uint64_t mapped[MPO_MAXW];
+    if (s->cfg.basis_rows != NULL) {
+        /* basis_change: the cutoff is judged on the image XOR_{slot s in P} row_s (change_basis,
+         * algebra/MajoranaAlgebra.h:179-189; MonomialPropagatorCommon.h:44-62), without the popcount fast
+         * path (AlgebraCommon.h:229-243 falls through to the stored function) */
+        for (int w = 0; w < W; ++w) mapped[w] = 0;
+        const int T2 = 64 * W;
+        for (int w = 0; w < W; ++w)
+            for (uint64_t x = p_in[w]; x; x &= x - 1) {
+                const int bit = 64 * w + __builtin_ctzll(x);
+                const int slot = T2 - 1 - bit;
+                for (int v = 0; v < W; ++v) mapped[v] ^= s->cfg.basis_rows[(size_t)slot * W + v];
+            }
+        p = mapped;
+        pop = 0;
+        for (int w = 0; w < W; ++w) pop += popc(mapped[w]);
+    }
     /* passes_with_popcount fast path is equivalent: measure <= popcount. */
     int xs = 0, os = 0;
     for (int w = 0; w < W; ++w) {

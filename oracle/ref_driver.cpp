@@ -73,7 +73,8 @@ template <size_t N>
 struct Impl final : Base {
     std::unique_ptr<MonomialPropagator<N>> p;
     std::optional<size_t> len_k;
-    Impl(const mpref_config &c, const OperatorDict &op, const VecZ &state) {
+    Impl(const mpref_config &c, const OperatorDict &op, const VecZ &state,
+         const std::optional<std::vector<VecZ>> &basis_change) {
         if (c.len_k > 0) len_k = static_cast<size_t>(c.len_k);
         std::optional<double> lo = c.has_lower ? std::optional<double>(c.lower) : std::nullopt;
         std::optional<double> hi = c.has_upper ? std::optional<double>(c.upper) : std::nullopt;
@@ -85,7 +86,7 @@ struct Impl final : Base {
                                                     lo,
                                                     hi,
                                                     c.cutoff_type == 1 ? CutoffType::Support : CutoffType::Length,
-                                                    std::nullopt,
+                                                    basis_change,
                                                     static_cast<size_t>(c.logical_num_modes),
                                                     c.basis == 1 ? Basis::Pauli : Basis::Majorana,
                                                     static_cast<size_t>(c.partitions));
@@ -138,6 +139,9 @@ void *mpref_create(const mpref_config *cfg,
                    const double *obs_im,
                    size_t n_state,
                    const int64_t *state,
+                   size_t n_basis,
+                   const int64_t *basis_off,
+                   const int64_t *basis_slots,
                    char *err,
                    size_t errlen) {
     try {
@@ -153,13 +157,20 @@ void *mpref_create(const mpref_config *cfg,
         for (size_t i = 0; i < n_state; ++i) {
             st.push_back(static_cast<size_t>(state[i]));
         }
+        std::optional<std::vector<VecZ>> basis;
+        if (n_basis > 0) {
+            basis.emplace(n_basis);
+            for (size_t r = 0; r < n_basis; ++r)
+                for (int64_t k = basis_off[r]; k < basis_off[r + 1]; ++k)
+                    (*basis)[r].push_back(static_cast<size_t>(basis_slots[k]));
+        }
         const int lm = cfg->logical_num_modes;
         const size_t tier = static_cast<size_t>((lm + 31) / 32) * 32;
         switch (tier) {
-        case 32: return new Impl<32>(*cfg, op, st);
-        case 64: return new Impl<64>(*cfg, op, st);
-        case 96: return new Impl<96>(*cfg, op, st);
-        case 128: return new Impl<128>(*cfg, op, st);
+        case 32: return new Impl<32>(*cfg, op, st, basis);
+        case 64: return new Impl<64>(*cfg, op, st, basis);
+        case 96: return new Impl<96>(*cfg, op, st, basis);
+        case 128: return new Impl<128>(*cfg, op, st, basis);
         default: set_err(err, errlen, "oracle driver built for at most 128 modes"); return nullptr;
         }
     }

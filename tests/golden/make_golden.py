@@ -14,6 +14,8 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
 * ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
   replayed graph;
 * ``<workload>_k<k>.npz`` -- seeded workloads propagated with ``only_rotate_len_k = k``;
+* ``<workload>_bc<pattern>.npz`` -- seeded Majorana workloads with a ``basis_change`` (written with the
+  ``only_rotate_len_k`` fixtures);
 * ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
   (``tests/data/{rx_rz_ry_rz_exact,random_exact,lih_fermionic_spin_exact}.msgpack``), re-expressed as
   engine arrays by this repository's front-end (``Circuit.from_dense_arrays`` + ``expand_monomials``,
@@ -39,6 +41,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
+from oracle import golden  # noqa: E402
 from monoprop_b200 import workloads as W  # noqa: E402
 from monoprop_b200.circuit import Circuit  # noqa: E402
 from monoprop_b200.encoding import canonical_order  # noqa: E402
@@ -59,7 +62,7 @@ SEEDED = [
 # only_rotate_len_k cases: (name, workload, layers, k)
 LEN_K = [
     ("line20_k6", W.line20, None, 6),
-    ("hubbard6x6_L400_k6", W.hubbard6x6, 400, 6),
+    ("hubbard6x6_L400_k4", W.hubbard6x6, 400, 4),
     ("ising50_d3_k8", lambda: W.ising50(3), None, 8),
 ]
 
@@ -125,6 +128,12 @@ def main(reference_root: str = "/root/reference") -> None:
         r = oracle.run_ref(wl, n_layers=L)
         save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
                     {"n_layers": np.int64(wl.n_layers if L is None else L), "only_rotate_len_k": np.int64(k)})
+        print(name, r.keys.shape[0], r.expectation)
+    for name in golden.BASIS_CHANGE:
+        wl, L = golden.basis_change_workload(name)
+        r = oracle.run_ref(wl, n_layers=L)
+        save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
+                    {"n_layers": np.int64(wl.n_layers if L is None else L)})
         print(name, r.keys.shape[0], r.expectation)
     if "--len-k-only" in sys.argv:
         return
