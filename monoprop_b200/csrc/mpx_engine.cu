@@ -133,7 +133,8 @@ struct mpx_engine {
     // Large blocks through the kept-block cache (dev_alloc). The batch runner turns it off for its
     // engines: with several engines growing at once, power-of-two classes and idle kept blocks crowd
     // the device, and a 96-instance gradient batch took 2x longer with them.
-    bool keep_blocks = true; // pair records the last recording forward pass needed (sizes the next log)
+    bool keep_blocks = true;
+    bool use_pdl = true; // programmatic dependent launch of the per-gate kernels // pair records the last recording forward pass needed (sizes the next log)
     bool use_graphs = true;
     bool small_path = true; // run small stores in one shared-memory block (mpx_small.cuh)
     std::string err;
@@ -306,14 +307,32 @@ void dev_free(mpx_engine *e, void *ptr) { dev_release(e->device, e->stream, ptr)
 
 // ----- kernel dispatch over (W, basis) ------------------------------------------------------------------
 
+// Launches `kernel` on the engine stream, with programmatic dependent launch unless profiling (the
+// kernel waits with griddepcontrol.wait before reading what the previous kernel wrote).
+template <typename... KArgs, typename... Args>
+void launch_dep(mpx_engine *e, void (*kernel)(KArgs...), Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(e->grid));
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = e->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    const bool pdl = e->use_pdl && !e->profile;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int W, int B, int EXT>
 void launch_gate_ext(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], e->stream);
-    k_sweep<W, B, false, EXT><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
-                                                                 e->fwd_tape, e->d_stats);
+    launch_dep(e, &k_sweep<W, B, false, EXT>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape,
+               e->d_stats);
     if (ev) cudaEventRecord(ev[1], e->stream);
-    k_resolve<W, B, false, (EXT & 1) != 0><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate,
-                                                                               step, e->tr, e->fwd_tape);
+    launch_dep(e, &k_resolve<W, B, false, (EXT & 1) != 0>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr,
+               e->fwd_tape);
     if (ev) cudaEventRecord(ev[2], e->stream);
 }
 

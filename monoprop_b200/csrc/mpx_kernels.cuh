@@ -35,6 +35,13 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
     return pos;
 }
 
+// Programmatic dependent launch (sm_90+): the sweep and the resolve let the next kernel of the stream be
+// scheduled as soon as they start, and that kernel reads only constant circuit data until it waits for
+// this grid's completion (and memory) with griddepcontrol.wait. Launched without the attribute, the wait
+// returns at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
 constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
@@ -85,14 +92,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
     __shared__ uint32_t s_qn;               // the block's queries so far
     __shared__ uint32_t s_red[kWarps];
     __shared__ uint32_t s_fold[kMaxFoldCols];
-    // the counters and the gate's fold columns are read together (one memory latency, not two)
+    pdl_trigger();
+    // the gate (constant circuit data) before the dependency wait, the counters after it
     const GateDesc &gd = gates[gate];
-    const uint32_t stall = cnt->stall;
-    const uint64_t n0 = cnt->n;
     const int n_fold = gd.n_fold;
     const uint32_t fcol = threadIdx.x < kMaxFoldCols ? gd.fold_cols[threadIdx.x] : 0u;
     const bool empty = gd.empty != 0, g_odd = gd.g_odd != 0;
     const uint32_t pivot_col = gd.pivot_col;
+    pdl_wait();
+    const uint32_t stall = cnt->stall;
+    const uint64_t n0 = cnt->n;
     if (stall != kNoStall) return;
     if (2 * n0 > st.cap) {
         // Not enough room for the worst case (every term appends its partner): stop here, untouched,
@@ -488,12 +497,14 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                                                      Trunc tr, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
     __shared__ unsigned long long s_base, s_rbase;
-    // counters, this block's query count and the gate are read together (one memory latency)
+    pdl_trigger();
+    // the gate (constant circuit data) before the dependency wait; counters and query count after it
     const GateDesc &gd = gates[gate];
+    const bool empty = gd.empty != 0;
+    pdl_wait();
     const uint32_t stall = cnt->stall;
     const uint64_t n0 = cnt->n0;
     const uint32_t total = sc.blk_q[blockIdx.x];
-    const bool empty = gd.empty != 0;
     if (stall != kNoStall) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
