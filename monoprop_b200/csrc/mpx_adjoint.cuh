@@ -95,6 +95,8 @@ __device__ __forceinline__ double block_sum(double v, double *s_red) {
 // After a replayed gate: the store size the forward pass reached after this step (appended partners
 // were looked up, not re-inserted).
 __global__ void k_replay_advance(Counters *__restrict__ cnt, const uint64_t *__restrict__ n_next, uint32_t step) {
+    pdl_trigger();
+    pdl_wait();
     if (threadIdx.x == 0 && blockIdx.x == 0 && cnt->stall == kNoStall) cnt->n = n_next[step];
 }
 
@@ -129,6 +131,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_pairs(Tape tp, const GateDesc *_
                                                        uint32_t step, double *__restrict__ lam,
                                                        uint32_t *__restrict__ done, double *__restrict__ grad) {
     __shared__ double s_red[kBlock / 32];
+    pdl_trigger();
+    pdl_wait();
     const uint64_t base = tp.p_base[step];
     const uint64_t cnt = tp.p_cnt[step];
     if (cnt == 0) return;
@@ -166,6 +170,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__
                                                       uint32_t step, double *__restrict__ lam,
                                                       uint32_t *__restrict__ done, double *__restrict__ grad) {
     __shared__ double s_red[kBlock / 32];
+    pdl_trigger();
+    pdl_wait();
     const uint64_t base = tp.u_base[step];
     const uint64_t cnt = tp.u_cnt[step];
     if (cnt == 0) return;
@@ -218,6 +224,8 @@ template <bool LOG>
 __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ coef, Frozen fz,
                                                           const GateDesc *__restrict__ gates, uint32_t gate,
                                                           uint32_t step, uint32_t *__restrict__ done, Tape tp) {
+    pdl_trigger();
+    pdl_wait();
     const uint64_t b = fz.p_begin[step], cnt = fz.p_count[step];
     const GateDesc &gd = gates[gate];
     const double C = gd.cosv, S = gd.sinv;

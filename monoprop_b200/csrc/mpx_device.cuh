@@ -45,6 +45,13 @@ struct Trunc {
     const uint64_t *basis_rows;
 };
 
+// Programmatic dependent launch (sm_90+): the per-gate kernels let the next kernel of the stream be
+// scheduled as soon as they start, and that kernel reads only constant circuit data until it waits for
+// the previous grid's completion (and memory) with griddepcontrol.wait. Launched without the attribute,
+// the wait returns at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Device counters, one set per engine.
 struct Counters {
     unsigned long long n; // live term count (grows during the resolve kernel)

@@ -310,10 +310,10 @@ void dev_free(mpx_engine *e, void *ptr) { dev_release(e->device, e->stream, ptr)
 // Launches `kernel` on the engine stream, with programmatic dependent launch unless profiling (the
 // kernel waits with griddepcontrol.wait before reading what the previous kernel wrote).
 template <typename... KArgs, typename... Args>
-void launch_dep(mpx_engine *e, void (*kernel)(KArgs...), Args... args) {
+void launch_dep_on(mpx_engine *e, unsigned grid, unsigned block, void (*kernel)(KArgs...), Args... args) {
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(static_cast<unsigned>(e->grid));
-    cfg.blockDim = dim3(kBlock);
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = e->stream;
     cudaLaunchAttribute attr[1];
@@ -323,6 +323,12 @@ void launch_dep(mpx_engine *e, void (*kernel)(KArgs...), Args... args) {
     cfg.attrs = pdl ? attr : nullptr;
     cfg.numAttrs = pdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// The per-gate grid of the engine (one resident wave of kBlock-thread blocks).
+template <typename... KArgs, typename... Args>
+void launch_dep(mpx_engine *e, void (*kernel)(KArgs...), Args... args) {
+    launch_dep_on(e, static_cast<unsigned>(e->grid), kBlock, kernel, args...);
 }
 
 template <int W, int B, int EXT>
@@ -363,16 +369,14 @@ void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_
     bool mapped = false;
     if constexpr (B == 0) {
         if (e->tr.basis_rows != nullptr) {
-            k_sweep<W, B, true, 2><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step,
-                                                                      e->tr, tp, e->d_stats);
+            launch_dep(e, &k_sweep<W, B, true, 2>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp, e->d_stats);
             mapped = true;
         }
     }
     if (!mapped)
-        k_sweep<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp,
-                                                               e->d_stats);
-    k_resolve<W, B, true><<<e->grid, kBlock, 0, e->stream>>>(e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
-    k_replay_advance<<<1, 32, 0, e->stream>>>(e->d_cnt, tp.n_next, step);
+        launch_dep(e, &k_sweep<W, B, true>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp, e->d_stats);
+    launch_dep(e, &k_resolve<W, B, true>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
+    launch_dep_on(e, 1, 32, &k_replay_advance, e->d_cnt, tp.n_next, step);
 }
 
 // Shared-memory capacity of the single-block path per key width: the largest power-of-two-friendly size
@@ -410,8 +414,8 @@ SmallFn pick_small(int W, int basis) {
 template <int W, bool LOG>
 void launch_frozen(mpx_engine *e, const GateDesc *d_desc, const Frozen &fz, uint32_t gate, uint32_t step, uint64_t n0,
                    uint32_t *done, const Tape &tp) {
-    k_frozen_pairs<LOG><<<e->grid, kBlock, 0, e->stream>>>(e->st.coef, fz, d_desc, gate, step, done, tp);
-    k_frozen_scan<W, LOG><<<e->grid, kBlock, 0, e->stream>>>(e->st, d_desc, gate, step, n0, done, tp);
+    launch_dep(e, &k_frozen_pairs<LOG>, e->st.coef, fz, d_desc, gate, step, done, tp);
+    launch_dep(e, &k_frozen_scan<W, LOG>, e->st, d_desc, gate, step, n0, done, tp);
 }
 
 using FrozenFn = void (*)(mpx_engine *, const GateDesc *, const Frozen &, uint32_t, uint32_t, uint64_t, uint32_t *,
@@ -818,7 +822,9 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
         }
     }
     const uint64_t gen0 = e->store_gen;
-    const bool graphable = e->use_graphs && !e->profile && cd.persistent && !used_small;
+    // A gradient's forward pass is not captured: its tape buffers are allocated per call, so a captured
+    // range would rarely match the next call's pointers and each miss would pay a new capture.
+    const bool graphable = e->use_graphs && !e->profile && cd.persistent && !used_small && e->fwd_tape.w_anti == nullptr;
     bool replayed = false;
     if (graphable) {
         for (const auto &g : e->graphs) {
@@ -1172,8 +1178,10 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         }
         for (uint64_t st = hi; st-- > lo;) {
             const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
-            k_adj_pairs<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
-            k_adj_undo<<<e->grid, kBlock, 0, e->stream>>>(tp, cd.d_desc, gate, static_cast<uint32_t>(st), lam, done, grad);
+            launch_dep(e, &k_adj_pairs, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
+                       done, grad);
+            launch_dep(e, &k_adj_undo, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
+                       done, grad);
         }
         e->launches += 5 * (hi - lo) + 1;
         MPX_CUDA_REL(cudaGetLastError());

@@ -35,13 +35,6 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
     return pos;
 }
 
-// Programmatic dependent launch (sm_90+): the sweep and the resolve let the next kernel of the stream be
-// scheduled as soon as they start, and that kernel reads only constant circuit data until it waits for
-// this grid's completion (and memory) with griddepcontrol.wait. Launched without the attribute, the wait
-// returns at once.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
 constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
@@ -354,6 +347,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
     __shared__ uint32_t s_nw[kWarps];
     __shared__ unsigned long long s_ubase[kWarps];
     __shared__ uint32_t s_fold[kMaxFoldCols];
+    pdl_trigger();
+    pdl_wait();
     const GateDesc &gd = gates[gate];
     if (gd.empty || n0 == 0) return;
     const int n_fold = gd.n_fold;
