@@ -7,9 +7,9 @@
 // export of evolved_operator (MonomialPropagator.inl:1099-1127).
 //
 // Scope: the Heisenberg picture -- propagate, and build_graph + expectation_value[_and_gradient](parameters)
-// over the engine's frozen structure (mpx_graph_*), with basis_change (Majorana) and, for propagate,
-// only_rotate_len_k. schrodinger_cutoff, only_rotate_len_k in build_graph, graph functionals with paring,
-// contract_partially and MPI communicators raise NotImplementedError.
+// over the engine's frozen structure (mpx_graph_*) and contract_partially, with basis_change (Majorana)
+// and, for propagate, only_rotate_len_k. schrodinger_cutoff, only_rotate_len_k in build_graph, graph
+// functionals with paring and MPI communicators raise NotImplementedError.
 #include <pybind11/complex.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -281,6 +281,32 @@ public:
         return {ev, grad};
     }
 
+    // contract_partially (MonomialPropagator.inl:1053-1097): the stored graph replayed at `parameters`, as
+    // raw coefficients in store order, core term excluded; with no parameters, the current coefficients.
+    // inplace consumes the graph: the engine keeps the replayed operator and a plain propagate may follow.
+    std::vector<double> contract_partially(const std::vector<double> &parameters, bool inplace) {
+        if (!parameters.empty()) {
+            if (circ_ == nullptr)
+                throw GraphStateConflict("contract_partially(parameters) needs a stored graph (build_graph)");
+            expectation_value(parameters); // the engine now holds the graph replayed at `parameters`
+        }
+        uint64_t n = 0;
+        check(mpx_size(e_, &n), e_);
+        std::vector<uint64_t> words(n * kWords);
+        std::vector<double> coefs(n);
+        uint64_t got = 0;
+        check(mpx_export(e_, words.data(), coefs.data(), n, &got), e_);
+        if (inplace && circ_ != nullptr) {
+            mpx_circuit_destroy(circ_);
+            circ_ = nullptr;
+            mapping_.clear();
+            gen_.clear();
+            n_params_ = 0;
+            gates_ = 0;
+        }
+        return coefs;
+    }
+
     size_t graph_layers() const { return circ_ != nullptr ? mapping_.size() : 0; }
     size_t n_gates() const { return circ_ != nullptr ? gates_ : 0; }
 
@@ -447,6 +473,7 @@ void bind(py::module_ &m) {
         .def("expectation_value_and_gradient", &P::expectation_value_and_gradient, py::arg("parameters"))
         .def("evolved_operator", &P::evolved_operator, py::arg("parameters"), py::arg("atol"))
         .def("size", &P::size)
+        .def("contract_partially", &P::contract_partially, py::arg("parameters"), py::arg("inplace"))
         .def("graph_size", [](P &) { return std::pair<size_t, size_t>(0, 0); })
         .def("graph_layers", &P::graph_layers)
         .def("n_gates", &P::n_gates)

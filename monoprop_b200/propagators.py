@@ -87,6 +87,14 @@ class MonomialPropagator:
     def graph_layers(self) -> int:
         return self._simulator.graph_layers()
 
+    def contract_partially(self, parameters=None, *, inplace: bool = True) -> np.ndarray:
+        """The stored graph replayed at ``parameters`` as raw coefficients (store order, core term
+        excluded); ``inplace`` consumes the graph (``monomial_propagator.py:478-510``)."""
+        coeffs = np.asarray(self._simulator.contract_partially(self._bind(parameters), inplace))
+        if inplace:
+            self._n_params = 0
+        return coeffs
+
     def gradient(self, parameters=None):
         return self.expectation_value_and_gradient(parameters)[1]
 

@@ -120,3 +120,27 @@ def test_graph_exact_energy_and_gradient(name):
         fd[i] = (ep - em) / (2 * eps)
         xk[i] = old
     assert np.allclose(mp4.grad(xk), fd, atol=1e-6)
+
+
+def test_contract_partially():
+    """contract_partially (monomial_propagator.py:478-510): the graph replayed at new parameters as raw
+    coefficients; inplace consumes the graph, after which a plain propagate is allowed."""
+    g = golden.load("ref_random_exact")
+    wl = golden.fixture_workload(g, "ref_random_exact")
+    circuit = Circuit.from_dense_arrays(wl.gate_slots, wl.gen_coeffs, wl.param_map, wl.num_modes, wl.params,
+                                        wl.initial_state)
+    op = MajoranaOperator(wl.observable, wl.num_modes)
+    mp = MajoranaPropagator(op, wl.initial_state, cutoff=4)
+    mp.build_graph(circuit)
+    theta = np.asarray(wl.params) * 0.7 + 0.05
+    coefs = mp.contract_partially(theta, inplace=False)
+    assert coefs.shape == (mp.size(),) and mp.graph_layers() > 0
+    ev = mp.expectation_value(theta)
+    evolved = mp.evolved_operator(theta, atol=0.0)
+    assert np.allclose(np.sort(np.abs(coefs)), np.sort([abs(c) for k, c in evolved.terms.items() if len(k)]),
+                       atol=1e-12)
+    again = mp.contract_partially(theta, inplace=True)
+    assert np.array_equal(np.sort(again), np.sort(coefs))
+    assert mp.graph_layers() == 0
+    assert abs(mp.expectation_value() - ev) <= 1e-12 * max(1.0, abs(ev))
+    mp.propagate(circuit)  # no graph left: a plain propagation continues from the contracted operator
