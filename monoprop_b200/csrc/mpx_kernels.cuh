@@ -8,7 +8,9 @@
 //   k_resolve -- one thread per emitted branch: open-addressing lookup of the partner M^G, the
 //                leader/follower rule, the rotation of the pair, or the unique append of the missing partner.
 //              It also ORs the appended terms' bits into the bit-columns.
-//   k_columns -- (re)builds the bit-columns of a range of stored terms (construction, growth, reset).
+//   k_columns -- builds the bit-columns of a range of stored terms (construction, reset, after the
+//                shared-memory path; a regrown store copies its column words instead).
+// The two per-gate kernels are launched with programmatic dependent launch (pdl_trigger / pdl_wait).
 // Every coefficient slot is written by exactly one thread per gate (the sine partner map M -> M^G is
 // injective), so no coefficient atomics are needed (layer_build/FusedApply.h:54-56).
 #pragma once
