@@ -305,6 +305,36 @@ void dev_release(int device, cudaStream_t stream, void *ptr) {
 
 void dev_free(mpx_engine *e, void *ptr) { dev_release(e->device, e->stream, ptr); }
 
+// Small pinned host buffers (counter snapshots, results) are reused across engines: cudaFreeHost waits
+// for the whole device, which in a batch would stall every other engine's stream once per instance.
+struct PinnedCache {
+    std::mutex mu;
+    std::map<size_t, std::vector<void *>> idle;
+};
+PinnedCache &pinned_cache() {
+    static PinnedCache *c = new PinnedCache; // never destroyed: engines may outlive static destruction
+    return *c;
+}
+cudaError_t pinned_get(void **ptr, size_t bytes) {
+    PinnedCache &c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.idle.find(bytes);
+        if (it != c.idle.end() && !it->second.empty()) {
+            *ptr = it->second.back();
+            it->second.pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaMallocHost(ptr, bytes);
+}
+void pinned_put(void *ptr, size_t bytes) {
+    if (ptr == nullptr) return;
+    PinnedCache &c = pinned_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.idle[bytes].push_back(ptr);
+}
+
 // ----- kernel dispatch over (W, basis) ------------------------------------------------------------------
 
 // Launches `kernel` on the engine stream, with programmatic dependent launch unless profiling (the
@@ -1518,21 +1548,26 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
         e->err = "cannot create the device memory pool";
         return bail(MPX_ERR_CUDA);
     }
-    cudaError_t ce = cudaMalloc(reinterpret_cast<void **>(&e->d_cnt), sizeof(Counters));
-    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_cnt), sizeof(Counters));
-    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
+    // Engine buffers come from the pool, stream-ordered, and pinned host buffers from a cache: creating and
+    // destroying an engine waits for no other stream (cudaMalloc / cudaFree would, device-wide).
+    cudaError_t ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_cnt), sizeof(Counters));
+    if (ce == cudaSuccess) ce = pinned_get(reinterpret_cast<void **>(&e->h_cnt), sizeof(Counters));
+    if (ce == cudaSuccess) ce = pinned_get(reinterpret_cast<void **>(&e->h_snap), 2 * sizeof(Counters));
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[0], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev[1], cudaEventDisableTiming);
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->sc.blk_q), e->grid * sizeof(uint32_t));
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
-    if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_out), sizeof(double));
-    if (ce == cudaSuccess) ce = cudaMallocHost(reinterpret_cast<void **>(&e->h_out), sizeof(double));
+    if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->sc.blk_q), e->grid * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
+    if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_out), sizeof(double));
+    if (ce == cudaSuccess) ce = pinned_get(reinterpret_cast<void **>(&e->h_out), sizeof(double));
     if (ce == cudaSuccess && n_obs > 0) {
-        ce = cudaMalloc(reinterpret_cast<void **>(&e->d_init_keys), n_obs * e->W * sizeof(uint64_t));
-        if (ce == cudaSuccess) ce = cudaMalloc(reinterpret_cast<void **>(&e->d_init_coef), n_obs * sizeof(double));
+        ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_keys), n_obs * e->W * sizeof(uint64_t));
+        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_coef), n_obs * sizeof(double));
         if (ce == cudaSuccess)
-            ce = cudaMemcpy(e->d_init_keys, obs_words, n_obs * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice);
-        if (ce == cudaSuccess) ce = cudaMemcpy(e->d_init_coef, obs_coef, n_obs * sizeof(double), cudaMemcpyHostToDevice);
+            ce = cudaMemcpyAsync(e->d_init_keys, obs_words, n_obs * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                 e->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(e->d_init_coef, obs_coef, n_obs * sizeof(double), cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream); // the caller's arrays may go away
     }
     if (ce != cudaSuccess) {
         e->err = std::string("CUDA setup failed: ") + cudaGetErrorString(ce);
@@ -1745,7 +1780,7 @@ mpx_status mpx_set_basis_change(mpx_engine *e, const uint64_t *rows, uint32_t n_
     if (rows == nullptr) return fail(e, MPX_ERR_INVALID, "basis_change rows are NULL");
     MPX_CUDA(cudaSetDevice(e->device));
     const size_t bytes = static_cast<size_t>(64 * e->W) * e->W * sizeof(uint64_t); // 2T rows of W words
-    if (e->d_basis == nullptr) MPX_CUDA(cudaMalloc(reinterpret_cast<void **>(&e->d_basis), bytes));
+    if (e->d_basis == nullptr) MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_basis), bytes));
     MPX_CUDA(cudaMemsetAsync(e->d_basis, 0, bytes, e->stream));
     MPX_CUDA(cudaMemcpyAsync(e->d_basis, rows, static_cast<size_t>(n_rows) * e->W * sizeof(uint64_t),
                              cudaMemcpyHostToDevice, e->stream));
@@ -1924,19 +1959,19 @@ void mpx_destroy(mpx_engine *e) {
     cudaStreamSynchronize(e->stream);
     clear_graphs(e);
     free_store(e);
-    cudaFree(e->d_cnt);
-    cudaFreeHost(e->h_cnt);
-    cudaFreeHost(e->h_snap);
+    dev_free(e, e->d_cnt);
+    pinned_put(e->h_cnt, sizeof(Counters));
+    pinned_put(e->h_snap, 2 * sizeof(Counters));
     for (auto &ev : e->ev)
         if (ev != nullptr) cudaEventDestroy(ev);
     for (auto &ev : e->pev) cudaEventDestroy(ev);
-    cudaFree(e->sc.blk_q);
-    cudaFree(e->d_partial);
-    cudaFree(e->d_out);
-    cudaFreeHost(e->h_out);
-    cudaFree(e->d_init_keys);
-    cudaFree(e->d_init_coef);
-    cudaFree(e->d_basis);
+    dev_free(e, e->sc.blk_q);
+    dev_free(e, e->d_partial);
+    dev_free(e, e->d_out);
+    pinned_put(e->h_out, sizeof(double));
+    dev_free(e, e->d_init_keys);
+    dev_free(e, e->d_init_coef);
+    dev_free(e, e->d_basis);
     dev_free(e, e->d_stats);
     if (e->stream != nullptr) {
         cudaStreamSynchronize(e->stream); // the pool frees above are stream-ordered
