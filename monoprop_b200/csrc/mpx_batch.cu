@@ -21,8 +21,9 @@
 
 #include "../../include/mpx.h"
 
-// Defined in mpx_engine.cu, not exported: engines of a batch allocate straight from the pool.
-extern "C" void mpx_internal_block_keeping(mpx_engine *e, int32_t on);
+// Defined in mpx_engine.cu, not exported: engines of a batch share the GPU (plain pool allocations, no
+// programmatic dependent launch).
+extern "C" void mpx_internal_shared_gpu(mpx_engine *e, int32_t shared);
 
 namespace {
 
@@ -45,7 +46,7 @@ mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_op
         err = mpx_last_error(nullptr);
         return s;
     }
-    mpx_internal_block_keeping(e, 0); // concurrent engines: plain pool allocations
+    mpx_internal_shared_gpu(e, 1); // concurrent engines
     mpx_circuit *c = nullptr;
     s = mpx_circuit_upload(e, it.gen_words, it.angles, it.n_layers, &c);
     if (s == MPX_OK) {

@@ -1941,9 +1941,13 @@ mpx_status mpx_trim_device_memory(int32_t device) {
     return MPX_OK;
 }
 
-// Internal (not exported): the batch runner's engines allocate straight from the pool.
-void mpx_internal_block_keeping(mpx_engine *e, int32_t on) {
-    if (e != nullptr) e->keep_blocks = on != 0;
+// Internal (not exported): the batch runner's engines allocate straight from the pool and launch
+// without programmatic dependent launch (with several engines' streams sharing the GPU, a kernel
+// scheduled early would hold SM slots at its dependency wait that another engine's ready kernel needs).
+void mpx_internal_shared_gpu(mpx_engine *e, int32_t shared) {
+    if (e == nullptr) return;
+    e->keep_blocks = shared == 0;
+    e->use_pdl = shared == 0;
 }
 
 const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }
