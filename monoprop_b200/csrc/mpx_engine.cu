@@ -352,7 +352,15 @@ void launch_dep_on(mpx_engine *e, unsigned grid, unsigned block, void (*kernel)(
     const bool pdl = e->use_pdl && !e->profile;
     cfg.attrs = pdl ? attr : nullptr;
     cfg.numAttrs = pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, kernel, args...);
+    if (cudaLaunchKernelEx(&cfg, kernel, args...) != cudaSuccess && pdl) {
+        // the attribute was refused: launch plainly from now on (a failed launch of the kernel itself
+        // fails again here and is reported by the caller's error check)
+        cudaGetLastError();
+        e->use_pdl = false;
+        cfg.attrs = nullptr;
+        cfg.numAttrs = 0;
+        cudaLaunchKernelEx(&cfg, kernel, args...);
+    }
 }
 
 // The per-gate grid of the engine (one resident wave of kBlock-thread blocks).

@@ -60,3 +60,20 @@ def test_autotuner_sample_is_depth_stratified():
     got = sorted(wl.n_layers for wl in sample)
     assert len(sample) == 8 and got[0] == depths[0] and got[-1] >= depths[len(depths) * 3 // 4]
     assert signature(batch).startswith("pauli-W2-c8-support")
+
+
+def test_basis_rows_encoding():
+    """basis_change rows: one row per slot, listed slots set once (indices_to_bitset_checked), zero rows
+    above 2 * num_modes, the reference's row-count message."""
+    import numpy as np
+    import pytest
+
+    from monoprop_b200.encoding import basis_rows, slots_to_words
+
+    n = 6
+    rows = basis_rows([[s] if s % 2 == 0 else [s - 1, s, s] for s in range(2 * n)], n)
+    assert rows.shape == (64, 1)
+    assert np.array_equal(rows[3], slots_to_words([2, 3], n))  # the duplicate 3 is set, not cancelled
+    assert not rows[2 * n:].any()
+    with pytest.raises(ValueError, match="basis_change must have exactly 2\\*logical_num_modes \\(12\\) rows"):
+        basis_rows([[0]] * 5, n)
