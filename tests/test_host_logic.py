@@ -77,3 +77,27 @@ def test_basis_rows_encoding():
     assert not rows[2 * n:].any()
     with pytest.raises(ValueError, match="basis_change must have exactly 2\\*logical_num_modes \\(12\\) rows"):
         basis_rows([[0]] * 5, n)
+
+
+def test_reference_arm_json_line():
+    """bench.py --impl reference: one JSON line on the bench's metric, with the reference-arm keys
+    (impl, cpu_baseline describing the run, e2e with no host-device bytes)."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    import pytest
+
+    import oracle
+
+    if not oracle.ref_available():
+        pytest.skip("reference oracle not built here")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--workload",
+                          "line20", "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])
+    assert d["impl"] == "reference" and d["metric"] == "term-gate updates/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
