@@ -45,14 +45,14 @@ class _PortCfg(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower", C.c_int32), ("lower", C.c_double), ("has_upper", C.c_int32),
                 ("upper", C.c_double), ("words", C.c_int32), ("has_len_k", C.c_int32), ("len_k", C.c_uint32),
-                ("basis_rows", C.c_void_p)]
+                ("basis_rows", C.c_void_p), ("schrodinger", C.c_int32), ("logical_modes", C.c_int32)]
 
 
 class _RefCfg(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower", C.c_int32), ("lower", C.c_double), ("has_upper", C.c_int32),
                 ("upper", C.c_double), ("partitions", C.c_int32), ("logical_num_modes", C.c_int32),
-                ("len_k", C.c_int32)]
+                ("len_k", C.c_int32), ("schrodinger_cutoff", C.c_int32)]
 
 
 _P = np.ctypeslib.ndpointer
@@ -152,7 +152,9 @@ def run_port(wl, params: np.ndarray | None = None, n_layers: int | None = None) 
     cfg = _PortCfg(_basis_code(wl.basis), _cutoff_code(wl.cutoff_type), wl.cutoff,
                    int(wl.lower_atol is not None), float(wl.lower_atol or 0.0),
                    int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), W,
-                   int(len_k is not None), int(len_k or 0), None if rows is None else rows.ctypes.data)
+                   int(len_k is not None), int(len_k or 0), None if rows is None else rows.ctypes.data,
+                   int(wl.extra["schrodinger_cutoff"]) if wl.extra.get("schrodinger_cutoff") is not None else -1,
+                   int(wl.num_modes))
     keys = np.ascontiguousarray(keys, dtype=np.uint64)
     coefs = np.ascontiguousarray(coefs, dtype=np.float64)
     mask = np.ascontiguousarray(wl.state_mask(), dtype=np.uint64)
@@ -202,7 +204,8 @@ class RefEngine:
         cfg = _RefCfg(_basis_code(wl.basis), _cutoff_code(wl.cutoff_type), wl.cutoff,
                       int(wl.lower_atol is not None), float(wl.lower_atol or 0.0),
                       int(wl.upper_atol is not None), float(wl.upper_atol or 0.0), partitions, wl.num_modes,
-                      int(wl.extra.get("only_rotate_len_k") or 0))
+                      int(wl.extra.get("only_rotate_len_k") or 0),
+                      int(wl.extra["schrodinger_cutoff"]) if wl.extra.get("schrodinger_cutoff") is not None else -1)
         err = C.create_string_buffer(1024)
         self._keep = (off, flat, re, im, st)
         bc = wl.extra.get("basis_change")

@@ -49,6 +49,21 @@ def basis_change_workload(name: str):
     return dataclasses.replace(wl, extra={**wl.extra, "basis_change": basis_pattern(kind, wl.num_modes)}), L
 
 
+#: seeded workloads in the Schrodinger picture: name -> (base workload name, layers, schrodinger_cutoff)
+SCHRODINGER = {"line20_L100_s4": ("line20", 100, 4), "hubbard6x6_L200_s4": ("hubbard6x6", 200, 4)}
+
+
+def schrodinger_workload(name: str):
+    """(workload with schrodinger_cutoff set, layers) of the ``SCHRODINGER`` fixture ``name``."""
+    import dataclasses
+
+    from monoprop_b200 import workloads as W
+
+    base, L, sc = SCHRODINGER[name]
+    wl = {"line20": W.line20, "hubbard6x6": W.hubbard6x6}[base]()
+    return dataclasses.replace(wl, extra={**wl.extra, "schrodinger_cutoff": sc}), L
+
+
 def len_k_workload(name: str):
     """(workload with only_rotate_len_k set, layers) of the ``LEN_K`` fixture ``name``."""
     import dataclasses

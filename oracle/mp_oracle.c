@@ -24,6 +24,10 @@
  *     adds (FusedApply.h:46-52, Engine.h:553,599-614).
  *   - basis_change: the structural cutoff of a partner is judged on its image under the given basis rows
  *     (algebra/MajoranaAlgebra.h:179-189, detail/monomial_propagator/MonomialPropagatorCommon.h:44-62).
+ *   - Schrodinger picture: the store starts as every fully paired monomial up to schrodinger_cutoff,
+ *     each holding its reference-state score; gates run first to last at the negated angle, a fresh
+ *     partner starts from its own score, and <O> is the observable dotted into the evolved state
+ *     (MonomialPropagator.inl:146-179,595-620; FusedApply.h:39-83; MPFunctions.cpp:196-205).
  *   - <0|O|0> = core + sum over fully paired rows of phase*c (MPOperator.h:235-254,
  *     algebra/PauliAlgebra.h:144-147, algebra/MajoranaAlgebra.h:56-60, MPFunctions.cpp:196-205).
  *
@@ -53,6 +57,9 @@ typedef struct {
     uint32_t len_k;
     /* basis_change: [2T][W] rows indexed by slot (rows of slots >= 2 * logical modes are zero), or NULL */
     const uint64_t *basis_rows;
+    /* Schrodinger picture (schrodinger >= 0: its cutoff) over `logical_modes` modes */
+    int32_t schrodinger;
+    int32_t logical_modes;
 } mpo_config;
 
 typedef struct {
@@ -66,6 +73,10 @@ typedef struct {
     uint32_t epoch;
     double core;
     uint64_t state_mask[MPO_MAXW];
+    /* Schrodinger picture: the observable, kept apart from the evolved state store */
+    size_t n_obs;
+    uint64_t *obs_keys;
+    double *obs_coef;
 } mpo_state;
 
 static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
@@ -196,6 +207,20 @@ static int is_paired(const uint64_t *p, int W) {
 
 static int nc2(int n) { return n * (n - 1) / 2; }
 
+/* <b|M|b> of the reference product state: the state phase of a fully paired row, else 0
+ * (MPOperator.h:235-254; PauliAlgebra.h:144-147; MajoranaAlgebra.h:56-60). */
+static double state_score(const mpo_state *s, const uint64_t *m) {
+    const int W = s->cfg.words;
+    if (!is_paired(m, W)) return 0.0;
+    int na = 0, pop = 0;
+    for (int w = 0; w < W; ++w) {
+        na += popc(m[w] & s->state_mask[w]);
+        pop += popc(m[w]);
+    }
+    const int odd = s->cfg.basis == 1 ? (na & 1) : ((na + pop / 2) & 1);
+    return odd ? -1.0 : 1.0;
+}
+
 typedef struct {
     uint64_t g[MPO_MAXW], fold[MPO_MAXW], wmask[MPO_MAXW];
     int gpop, gy, g_odd, pivot_word;
@@ -278,8 +303,49 @@ void *mpo_create(const mpo_config *cfg,
     s->cfg = *cfg;
     s->core = core;
     memcpy(s->state_mask, state_mask, sizeof(uint64_t) * cfg->words);
-    if (reserve(s, n_terms ? n_terms : 1) != 0) return NULL;
     const int W = cfg->words;
+    if (cfg->schrodinger >= 0) {
+        /* Schrodinger picture (MonomialPropagator.inl:146-179): the store starts as every fully paired
+         * monomial of at most K = sc/2 + sc%2 pairs over the logical modes, sc = min(schrodinger_cutoff,
+         * 2 * modes) (generate_paired_op, MajoranaAlgebra.h:127-160), each holding its reference-state
+         * score; the observable is kept apart for the final dot product. */
+        s->n_obs = n_terms;
+        s->obs_keys = malloc(sizeof(uint64_t) * W * (n_terms ? n_terms : 1));
+        s->obs_coef = malloc(sizeof(double) * (n_terms ? n_terms : 1));
+        if (!s->obs_keys || !s->obs_coef) return NULL;
+        memcpy(s->obs_keys, words, sizeof(uint64_t) * W * n_terms);
+        memcpy(s->obs_coef, coefs, sizeof(double) * n_terms);
+        const int L = cfg->logical_modes;
+        int sc = cfg->schrodinger;
+        if (sc > 2 * L) sc = 2 * L;
+        int K = sc / 2 + sc % 2;
+        if (K > L) K = L;
+        int sel[256];
+        for (int k = 0; k <= K; ++k) {
+            /* subsets of k modes in lexicographic order */
+            for (int i = 0; i < k; ++i) sel[i] = i;
+            for (;;) {
+                if (reserve(s, s->n + 1) != 0) return NULL;
+                uint64_t *m = s->keys + s->n * W;
+                memset(m, 0, sizeof(uint64_t) * W);
+                for (int i = 0; i < k; ++i)
+                    for (int slot = 2 * sel[i]; slot <= 2 * sel[i] + 1; ++slot) {
+                        const int bit = 64 * W - 1 - slot;
+                        m[bit / 64] |= 1ULL << (bit % 64);
+                    }
+                s->coef[s->n] = state_score(s, m);
+                table_put(s, s->n);
+                s->n++;
+                int i = k - 1;
+                while (i >= 0 && sel[i] == L - k + i) --i;
+                if (i < 0) break;
+                ++sel[i];
+                for (int j = i + 1; j < k; ++j) sel[j] = sel[j - 1] + 1;
+            }
+        }
+        return s;
+    }
+    if (reserve(s, n_terms ? n_terms : 1) != 0) return NULL;
     for (size_t i = 0; i < n_terms; ++i) {
         memcpy(s->keys + s->n * W, words + i * W, sizeof(uint64_t) * W);
         s->coef[s->n] = coefs[i];
@@ -298,10 +364,13 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
     query *qs = NULL;
     size_t qcap = 0;
     size_t *miss = NULL;
+    const int schr = s->cfg.schrodinger >= 0;
     for (size_t step = 0; step < n_gates; ++step) {
-        const size_t gi = n_gates - 1 - step;
+        /* Heisenberg: last gate first; Schrodinger: first gate first at the negated angle
+         * (MonomialPropagator.inl:720-733, map_params with phase -1, MPFunctions.cpp:186-193) */
+        const size_t gi = schr ? step : n_gates - 1 - step;
         const uint64_t *g = gen_words + gi * W;
-        const double ang = angles[gi];
+        const double ang = schr ? -angles[gi] : angles[gi];
         const double cosv = cos(2.0 * ang);
         const double sinv = sin(2.0 * ang);
         const double abs_sin = fabs(sinv);
@@ -403,7 +472,23 @@ int mpo_propagate(void *hs, size_t n_gates, const uint64_t *gen_words, const dou
             const query *q = &qs[miss[k]];
             const size_t idx = s->n++;
             memcpy(s->keys + idx * W, q->p, sizeof(uint64_t) * W);
-            c_arr[idx] = sinv * (double)q->phase * q->v;
+            if (schr) {
+                /* a fresh slot starts from its reference-state score, and the pair rotates as a hit does
+                 * (FusedApply.h:39-83: v_tgt read after the extension; cos folded in for the new slot) */
+                const double vt = state_score(s, q->p);
+                c_arr[q->src] += sinv * (double)(-q->phase) * vt;
+                if (fused) {
+                    c_arr[idx] = vt;
+                    c_arr[idx] = cosv * c_arr[idx] + sinv * (double)q->phase * q->v;
+                }
+                else {
+                    c_arr[idx] = cosv * vt;
+                    c_arr[idx] += sinv * (double)q->phase * q->v;
+                }
+            }
+            else {
+                c_arr[idx] = sinv * (double)q->phase * q->v;
+            }
             table_put(s, idx);
         }
         free(hits);
@@ -431,6 +516,14 @@ double mpo_expectation(void *hs) {
     mpo_state *s = hs;
     const int W = s->cfg.words;
     double acc = 0.0;
+    if (s->cfg.schrodinger >= 0) {
+        /* Schrodinger: core + state . observable over the stored rows (MPFunctions.cpp:196-205) */
+        for (size_t t = 0; t < s->n_obs; ++t) {
+            const size_t j = find(s, s->obs_keys + t * W);
+            if (j != SIZE_MAX) acc += s->obs_coef[t] * s->coef[j];
+        }
+        return s->core + acc;
+    }
     for (size_t i = 0; i < s->n; ++i) {
         const uint64_t *m = s->keys + i * W;
         if (!is_paired(m, W)) continue;
@@ -452,5 +545,7 @@ void mpo_destroy(void *hs) {
     free(s->coef);
     free(s->table);
     free(s->mark);
+    free(s->obs_keys);
+    free(s->obs_coef);
     free(s);
 }

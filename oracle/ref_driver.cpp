@@ -32,6 +32,7 @@ struct mpref_config {
     int32_t partitions;        // >= 1
     int32_t logical_num_modes; // modes (Majorana) or qubits (Pauli)
     int32_t len_k;             // only_rotate_len_k, 0 = not given
+    int32_t schrodinger_cutoff; // < 0: Heisenberg picture; >= 0: the Schrodinger picture with this cutoff
 };
 }
 
@@ -78,10 +79,12 @@ struct Impl final : Base {
         if (c.len_k > 0) len_k = static_cast<size_t>(c.len_k);
         std::optional<double> lo = c.has_lower ? std::optional<double>(c.lower) : std::nullopt;
         std::optional<double> hi = c.has_upper ? std::optional<double>(c.upper) : std::nullopt;
+        std::optional<unsigned int> sc;
+        if (c.schrodinger_cutoff >= 0) sc = static_cast<unsigned int>(c.schrodinger_cutoff);
         p = std::make_unique<MonomialPropagator<N>>(op,
                                                     c.cutoff,
                                                     state,
-                                                    std::nullopt,
+                                                    sc,
                                                     mpi::Comm{},
                                                     lo,
                                                     hi,

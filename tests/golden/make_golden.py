@@ -14,7 +14,8 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
 * ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
   replayed graph;
 * ``<workload>_k<k>.npz`` -- seeded workloads propagated with ``only_rotate_len_k = k``;
-* ``<workload>_bc<pattern>.npz`` -- seeded Majorana workloads with a ``basis_change`` (written with the
+* ``<workload>_bc<pattern>.npz`` -- seeded Majorana workloads with a ``basis_change``, and
+  ``<workload>_s<cutoff>.npz`` -- seeded workloads in the Schrodinger picture (both written with the
   ``only_rotate_len_k`` fixtures);
 * ``ref_<case>.npz`` -- the reference's own exact-energy test fixtures
   (``tests/data/{rx_rz_ry_rz_exact,random_exact,lih_fermionic_spin_exact}.msgpack``), re-expressed as
@@ -128,6 +129,12 @@ def main(reference_root: str = "/root/reference") -> None:
         r = oracle.run_ref(wl, n_layers=L)
         save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
                     {"n_layers": np.int64(wl.n_layers if L is None else L), "only_rotate_len_k": np.int64(k)})
+        print(name, r.keys.shape[0], r.expectation)
+    for name in golden.SCHRODINGER:
+        wl, L = golden.schrodinger_workload(name)
+        r = oracle.run_ref(wl, n_layers=L)
+        save_result(os.path.join(HERE, name + ".npz"), r.keys, r.coefs, r.expectation,
+                    {"n_layers": np.int64(wl.n_layers if L is None else L)})
         print(name, r.keys.shape[0], r.expectation)
     for name in golden.BASIS_CHANGE:
         wl, L = golden.basis_change_workload(name)

@@ -7,7 +7,8 @@
   (random Pauli and Majorana circuits exercising lower_atol, upper_atol rescue, odd-weight generators,
   near-zero cosines and the fully-paired exemption);
 * on the analytic one-gate truncation cases of the reference's tests/test_coeff_trunc.py:59-96;
-* with only_rotate_len_k and with a basis_change, against golden fixtures and the live reference.
+* with only_rotate_len_k, with a basis_change and in the Schrodinger picture, against golden fixtures
+  and the live reference.
 """
 
 import dataclasses
@@ -98,6 +99,27 @@ def test_port_matches_reference_live_basis_change(seed, kind):
     assert np.array_equal(a.keys[ia], b.keys[ib])
     assert np.array_equal(a.coefs[ia], b.coefs[ib])
     assert a.expectation == b.expectation
+
+
+@pytest.mark.parametrize("name", sorted(golden.SCHRODINGER))
+def test_port_matches_reference_golden_schrodinger(name):
+    """Schrodinger picture: paired-monomial state evolved first to last at the negated angle."""
+    wl, L = golden.schrodinger_workload(name)
+    r = oracle.run_port(wl, n_layers=L)
+    golden.check_against(golden.load(name), r.keys, r.coefs, r.expectation)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built here")
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("basis", ["pauli", "majorana"])
+def test_port_matches_reference_live_schrodinger(seed, basis):
+    base = random_workload(seed, basis)
+    wl = dataclasses.replace(base, extra={**base.extra, "schrodinger_cutoff": base.cutoff + 1})
+    a, b = oracle.run_port(wl), oracle.run_ref(wl)
+    ia, ib = canonical_order(a.keys), canonical_order(b.keys)
+    assert np.array_equal(a.keys[ia], b.keys[ib])
+    assert np.array_equal(a.coefs[ia], b.coefs[ib])
+    assert abs(a.expectation - b.expectation) <= 1e-12 * max(1.0, abs(b.expectation))  # summation order
 
 
 def one_gate(cutoff, upper_atol, lower_atol):
