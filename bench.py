@@ -35,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -63,7 +64,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mpx_clocks_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:
@@ -416,7 +417,7 @@ def batch_bench(args) -> None:
     batch = full[rank::world]
     seg = 4 * 135
     run_batch(batch[-4:], BatchConfig(), gradient=True, segment_gates=seg, device=local)  # warm-up
-    tuner = Autotuner(cache_path=os.path.join(ROOT, "gpurun_out", "autotune.json"))
+    tuner = Autotuner(cache_path=os.path.join(tempfile.gettempdir(), f"mpx_autotune_{os.getpid()}.json"))
     t0 = time.perf_counter()
     best, entry = tuner.tune(batch, gradient=True, segment_gates=seg, device=local, use_cache=False)
     tune_s = time.perf_counter() - t0

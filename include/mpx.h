@@ -173,6 +173,12 @@ typedef struct {
     double *expectation;  /* out */
     double *grad_angles;  /* out [n_layers], or NULL */
     uint64_t *final_terms; /* out (store size after propagation), or NULL */
+    /* optional raw export of the evolved store, as mpx_export (NULL = none): up to export_cap keys
+     * [export_cap][W] and coefficients in storage order; *export_n = the store size */
+    uint64_t *export_words;
+    double *export_coefs;
+    uint64_t export_cap;
+    uint64_t *export_n;
 } mpx_batch_item;
 
 typedef struct {
@@ -234,7 +240,9 @@ MPX_API const char *mpx_last_error(const mpx_engine *e);
  * 268435456 (larger stores return MPX_ERR_CAPACITY). The first call on each device does a one-time
  * set-up: it looks the array up with cudaGetSymbolAddress, so that device must be current, and that first
  * call should come before any stream capture on the device begins. Every call shares the one array: calls whose
- * kernels may overlap on the GPU must be serialised by the caller. On failure a message is written to
+ * kernels may overlap on the GPU must be serialised by the caller. The status covers this call's own
+ * launches only (an error pending from the caller's earlier work is neither returned nor cleared); faults
+ * during execution surface at the caller's next synchronisation. On failure a message is written to
  * err (up to err_len bytes, NUL-terminated) when err is not NULL. */
 MPX_API mpx_status mpx_expectation_noalloc(int32_t basis, uint32_t words, const uint64_t *keys, const double *coefs,
                                            uint64_t n_terms, const uint64_t *state_mask, double core, double *out,

@@ -28,7 +28,8 @@ class _Item(C.Structure):
     _fields_ = [("obs_words", C.c_void_p), ("obs_coef", C.c_void_p), ("n_obs", C.c_uint64), ("core", C.c_double),
                 ("state_mask", C.c_void_p), ("gen_words", C.c_void_p), ("angles", C.c_void_p),
                 ("n_layers", C.c_uint64), ("expectation", C.c_void_p), ("grad_angles", C.c_void_p),
-                ("final_terms", C.c_void_p)]
+                ("final_terms", C.c_void_p), ("export_words", C.c_void_p), ("export_coefs", C.c_void_p),
+                ("export_cap", C.c_uint64), ("export_n", C.c_void_p)]
 
 
 class _Options(C.Structure):
@@ -51,11 +52,15 @@ class BatchResult:
     grads: list[np.ndarray] | None  # d<O>/d(angle_l) per instance (gradient runs)
     final_terms: np.ndarray
     seconds: float
+    exports: list[tuple[np.ndarray, np.ndarray]] | None = None  # raw (keys, coefs) per instance, on request
 
 
 def run_batch(workloads, config: BatchConfig | None = None, gradient: bool = False, segment_gates: int = 0,
-              device: int = 0) -> BatchResult:
-    """Propagate every workload (and its adjoint gradient when ``gradient``) in one engine call."""
+              device: int = 0, export_caps=None) -> BatchResult:
+    """Propagate every workload (and its adjoint gradient when ``gradient``) in one engine call.
+
+    ``export_caps``: per instance, the number of terms of room for a raw export of its evolved store
+    (keys and coefficients in storage order); the result's ``exports`` then holds them."""
     config = config or BatchConfig()
     lib = _native.load()
     if not workloads:
@@ -75,6 +80,10 @@ def run_batch(workloads, config: BatchConfig | None = None, gradient: bool = Fal
     ev = np.zeros(n, dtype=np.float64)
     terms = np.zeros(n, dtype=np.uint64)
     grads = [np.zeros(wl.n_layers, dtype=np.float64) for wl in workloads] if gradient else None
+    exp_bufs = None
+    if export_caps is not None:
+        exp_bufs = [(np.zeros((max(int(c), 1), w0.words), np.uint64), np.zeros(max(int(c), 1)), np.zeros(1, np.uint64))
+                    for c in export_caps]
     for i, wl in enumerate(workloads):
         keys, coefs, core = wl.encoded_observable()
         arrs = (np.ascontiguousarray(keys, np.uint64), np.ascontiguousarray(coefs, np.float64),
@@ -89,6 +98,10 @@ def run_batch(workloads, config: BatchConfig | None = None, gradient: bool = Fal
         it.expectation = ev.ctypes.data + 8 * i
         it.final_terms = terms.ctypes.data + 8 * i
         it.grad_angles = grads[i].ctypes.data if gradient and wl.n_layers else None
+        if exp_bufs is not None:
+            kb, cb, nb = exp_bufs[i]
+            it.export_words, it.export_coefs, it.export_n = kb.ctypes.data, cb.ctypes.data, nb.ctypes.data
+            it.export_cap = int(export_caps[i])
     opt = _Options(int(config.workers), int(gradient), int(segment_gates))
     err = C.create_string_buffer(1024)
     t0 = time.perf_counter()
@@ -96,7 +109,13 @@ def run_batch(workloads, config: BatchConfig | None = None, gradient: bool = Fal
     dt = time.perf_counter() - t0
     if rc != 0:
         raise _native.MpxError(rc, err.value.decode())
-    return BatchResult(ev, grads, terms, dt)
+    exports = None
+    if exp_bufs is not None:
+        exports = []
+        for (kb, cb, nb), cap in zip(exp_bufs, export_caps):
+            k = min(int(nb[0]), int(cap))
+            exports.append((kb[:k], cb[:k]))
+    return BatchResult(ev, grads, terms, dt, exports)
 
 
 def signature(workloads) -> str:

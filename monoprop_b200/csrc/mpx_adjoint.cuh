@@ -125,17 +125,29 @@ __global__ void __launch_bounds__(kBlock) k_adj_init(const uint64_t *__restrict_
     }
 }
 
+// dE/dangle of one gate is summed in a fixed order, so the gradient's bits do not depend on block
+// scheduling: every block of the two reverse-step kernels writes its partial sum to its own slot
+// (pairs kernel: slots [0, grid), undo kernel: [grid, 2 grid)), and the last undo block to finish (one
+// counter bump per block) adds all 2 grid partials in slot order and writes the gate's derivative.
+struct GradPartials {
+    double *part;           // [2 * grid]
+    unsigned int *arrivals; // undo blocks finished for the current gate; reset to 0 by the last one
+};
+
 // Reverse step, part 1: the gate's rotated and appended pairs. Writes lambda of both endpoints, marks
-// them in `done` (the undo pass skips them) and adds their share of dE/dangle.
+// them in `done` (the undo pass skips them) and stores this block's share of dE/dangle.
 __global__ void __launch_bounds__(kBlock) k_adj_pairs(Tape tp, const GateDesc *__restrict__ gates, uint32_t gate,
                                                        uint32_t step, double *__restrict__ lam,
-                                                       uint32_t *__restrict__ done, double *__restrict__ grad) {
+                                                       uint32_t *__restrict__ done, GradPartials gp) {
     __shared__ double s_red[kBlock / 32];
     pdl_trigger();
     pdl_wait();
     const uint64_t base = tp.p_base[step];
     const uint64_t cnt = tp.p_cnt[step];
-    if (cnt == 0) return;
+    if (cnt == 0) {
+        if (threadIdx.x == 0) gp.part[blockIdx.x] = 0.0;
+        return;
+    }
     const GateDesc &gd = gates[gate];
     const double C = gd.cosv, S = gd.sinv;
     double acc = 0.0;
@@ -160,21 +172,23 @@ __global__ void __launch_bounds__(kBlock) k_adj_pairs(Tape tp, const GateDesc *_
         }
     }
     const double t = block_sum(acc, s_red);
-    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&grad[gate], t);
+    if (threadIdx.x == 0) gp.part[blockIdx.x] = t;
 }
 
 // Reverse step, part 2: every anticommuting term of the gate. Terms not in a pair were only cos-scaled:
 // dE/dangle += lambda' (-2 s c_pre), lambda = C lambda'. Pair members were handled by part 1; their
 // done bit is cleared here (each appears once in the undo log), so `done` is all zero between gates.
+// The last block to finish writes grad[gate], the fixed-order sum of both kernels' partials.
 __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__restrict__ gates, uint32_t gate,
                                                       uint32_t step, double *__restrict__ lam,
-                                                      uint32_t *__restrict__ done, double *__restrict__ grad) {
+                                                      uint32_t *__restrict__ done, GradPartials gp,
+                                                      double *__restrict__ grad) {
     __shared__ double s_red[kBlock / 32];
+    __shared__ bool s_last;
     pdl_trigger();
     pdl_wait();
     const uint64_t base = tp.u_base[step];
     const uint64_t cnt = tp.u_cnt[step];
-    if (cnt == 0) return;
     const GateDesc &gd = gates[gate];
     const double C = gd.cosv, S = gd.sinv;
     double acc = 0.0;
@@ -195,7 +209,22 @@ __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__
         }
     }
     const double t = block_sum(acc, s_red);
-    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&grad[gate], t);
+    if (threadIdx.x == 0) {
+        gp.part[gridDim.x + blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(gp.arrivals, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    // every partial of this gate is written and visible (each writer fenced before its arrival)
+    __threadfence();
+    double v = 0.0;
+    for (uint32_t k = threadIdx.x; k < 2 * gridDim.x; k += blockDim.x) v += __ldcg(gp.part + k);
+    const double total = block_sum(v, s_red);
+    if (threadIdx.x == 0) {
+        grad[gate] = total;
+        *gp.arrivals = 0u;
+    }
 }
 
 }  // namespace mpx

@@ -21,9 +21,11 @@
 
 #include "../../include/mpx.h"
 
-// Defined in mpx_engine.cu, not exported: engines of a batch share the GPU (plain pool allocations, no
-// programmatic dependent launch).
-extern "C" void mpx_internal_shared_gpu(mpx_engine *e, int32_t shared);
+// Defined in mpx_engine.cu, not exported: mpx_create for an engine that shares the GPU with other
+// engines of a batch (plain pool allocations from its first buffer on, no programmatic dependent launch).
+extern "C" mpx_status mpx_internal_create_shared(const mpx_config *cfg, const uint64_t *obs_words,
+                                                 const double *obs_coef, uint64_t n_obs, double core,
+                                                 const uint64_t *state_mask, mpx_engine **out);
 
 namespace {
 
@@ -41,12 +43,11 @@ struct BatchState {
 // One instance on a fresh engine (the device memory pool makes engine creation cheap).
 mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_options &opt, std::string &err) {
     mpx_engine *e = nullptr;
-    mpx_status s = mpx_create(&cfg, it.obs_words, it.obs_coef, it.n_obs, it.core, it.state_mask, &e);
+    mpx_status s = mpx_internal_create_shared(&cfg, it.obs_words, it.obs_coef, it.n_obs, it.core, it.state_mask, &e);
     if (s != MPX_OK) {
         err = mpx_last_error(nullptr);
         return s;
     }
-    mpx_internal_shared_gpu(e, 1); // concurrent engines
     mpx_circuit *c = nullptr;
     s = mpx_circuit_upload(e, it.gen_words, it.angles, it.n_layers, &c);
     if (s == MPX_OK) {
@@ -59,6 +60,8 @@ mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_op
             if (s == MPX_OK) s = mpx_expectation(e, it.expectation);
         }
         if (s == MPX_OK && it.final_terms != nullptr) s = mpx_size(e, it.final_terms);
+        if (s == MPX_OK && it.export_n != nullptr)
+            s = mpx_export(e, it.export_words, it.export_coefs, it.export_cap, it.export_n);
     }
     if (s != MPX_OK) err = mpx_last_error(e);
     mpx_circuit_destroy(c);
@@ -68,8 +71,14 @@ mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_op
 
 void worker(const mpx_config &cfg, mpx_batch_item *items, const std::vector<uint64_t> &order,
             const mpx_batch_options &opt, BatchState &bs) {
-    if (cudaSetDevice(cfg.device) != cudaSuccess) {
+    if (const cudaError_t ce = cudaSetDevice(cfg.device); ce != cudaSuccess) {
         cudaGetLastError();
+        std::lock_guard<std::mutex> lock(bs.mu);
+        if (!bs.failed.exchange(true)) {
+            bs.status = MPX_ERR_CUDA;
+            bs.error = "cannot select device " + std::to_string(cfg.device) + ": " + cudaGetErrorString(ce);
+        }
+        bs.cv.notify_all();
         return;
     }
     for (;;) {
@@ -133,6 +142,14 @@ MPX_API mpx_status mpx_batch_run(const mpx_config *cfg, mpx_batch_item *items, u
             (it.n_obs > 0 && (it.obs_words == nullptr || it.obs_coef == nullptr)))
             return report(MPX_ERR_INVALID, "batch item " + std::to_string(i) + " has a NULL buffer");
     }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return report(MPX_ERR_NO_DEVICE, "no CUDA device is visible; the engine has no CPU fallback");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev)
+        return report(MPX_ERR_INVALID, "device ordinal " + std::to_string(cfg->device) + " out of range (" +
+                                           std::to_string(ndev) + " devices)");
     // deepest first: the longest instances start early, short ones fill in around them
     std::vector<uint64_t> order(n_items);
     std::iota(order.begin(), order.end(), 0);

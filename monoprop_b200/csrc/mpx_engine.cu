@@ -127,14 +127,14 @@ struct mpx_engine {
     };
     std::vector<GraphEntry> graphs;
     uint64_t store_gen = 0;
-    uint64_t rec_hint = 0;
+    uint64_t rec_hint = 0; // pair records the last recording forward pass needed (sizes the next log)
     int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity
     uint64_t *d_basis = nullptr; // basis_change rows [2T][W] (tr.basis_rows points here when set)
     // Large blocks through the kept-block cache (dev_alloc). The batch runner turns it off for its
     // engines: with several engines growing at once, power-of-two classes and idle kept blocks crowd
     // the device, and a 96-instance gradient batch took 2x longer with them.
     bool keep_blocks = true;
-    bool use_pdl = true; // programmatic dependent launch of the per-gate kernels // pair records the last recording forward pass needed (sizes the next log)
+    bool use_pdl = true; // programmatic dependent launch of the per-gate kernels
     bool use_graphs = true;
     bool small_path = true; // run small stores in one shared-memory block (mpx_small.cuh)
     std::string err;
@@ -854,6 +854,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             c.n = n;
             c.n0 = n;
             c.stall = kNoStall;
+            c.err = e->h_cnt->err; // a table inconsistency of the shared-memory path is reported below
             MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
             step = resume;
             used_small = true;
@@ -1128,6 +1129,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     uint64_t *d_steps = nullptr;  // u_base | p_base | n_next
     unsigned long long *d_cnts = nullptr; // u_cnt | p_cnt
     double *lam = nullptr, *grad = nullptr;
+    double *gpart = nullptr; // per-block partials of dE/dangle, then the arrival counter (GradPartials)
     uint32_t *done = nullptr;
     cudaError_t ce = cudaSuccess;
     auto A_ = [&](void **ptr, size_t bytes) {
@@ -1145,11 +1147,13 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     A_(reinterpret_cast<void **>(&lam), nf * sizeof(double));
     A_(reinterpret_cast<void **>(&grad), L * sizeof(double));
     A_(reinterpret_cast<void **>(&done), ((nf + 31) / 32) * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&gpart), (2 * static_cast<size_t>(e->grid) + 1) * sizeof(double));
     auto release = [&]() {
         for (void *ptr : {static_cast<void *>(tp.u_idx), static_cast<void *>(tp.u_val), static_cast<void *>(tp.p_src),
                           static_cast<void *>(tp.p_tgt), static_cast<void *>(tp.p_code), static_cast<void *>(tp.p_vs),
                           static_cast<void *>(tp.p_vt), static_cast<void *>(d_steps), static_cast<void *>(d_cnts),
-                          static_cast<void *>(lam), static_cast<void *>(grad), static_cast<void *>(done)})
+                          static_cast<void *>(lam), static_cast<void *>(grad), static_cast<void *>(done),
+                          static_cast<void *>(gpart)})
             dev_free(e, ptr);
     };
     if (ce != cudaSuccess) {
@@ -1189,6 +1193,8 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     tp.u_off = u_off;
     MPX_CUDA_REL(cudaMemsetAsync(grad, 0, L * sizeof(double), e->stream));
     MPX_CUDA_REL(cudaMemsetAsync(done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+    const GradPartials gp{gpart, reinterpret_cast<unsigned int *>(gpart + 2 * static_cast<size_t>(e->grid))};
+    MPX_CUDA_REL(cudaMemsetAsync(gp.arrivals, 0, sizeof(unsigned int), e->stream));
     pick_adj_init(e->W, e->cfg.basis)(e, lam, nf);
     const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
     const FrozenFn frozen_replay = pick_frozen<true>(e->W);
@@ -1217,9 +1223,9 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         for (uint64_t st = hi; st-- > lo;) {
             const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
             launch_dep(e, &k_adj_pairs, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
-                       done, grad);
+                       done, gp);
             launch_dep(e, &k_adj_undo, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
-                       done, grad);
+                       done, gp, grad);
         }
         e->launches += 5 * (hi - lo) + 1;
         MPX_CUDA_REL(cudaGetLastError());
@@ -1507,8 +1513,16 @@ mpx_status validate_cfg(const mpx_config *c) {
 
 extern "C" {
 
-mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef, uint64_t n_obs,
-                      double core, const uint64_t *state_mask, mpx_engine **out) {
+}  // extern "C"
+
+namespace {
+
+// mpx_create; `shared`: the engine shares the GPU with the other engines of a batch, so from its first
+// buffer on it allocates straight from the pool (no kept-block cache) and launches without programmatic
+// dependent launch (a kernel scheduled early would hold SM slots at its dependency wait that another
+// engine's ready kernel could use).
+mpx_status create_engine(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef, uint64_t n_obs,
+                         double core, const uint64_t *state_mask, mpx_engine **out, bool shared) {
     if (out == nullptr) return fail(nullptr, MPX_ERR_INVALID, "out is NULL");
     *out = nullptr;
     mpx_status s = validate_cfg(cfg);
@@ -1528,6 +1542,8 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     auto *e = new (std::nothrow) mpx_engine();
     if (e == nullptr) return fail(nullptr, MPX_ERR_NOMEM, "host allocation failed");
     e->cfg = *cfg;
+    e->keep_blocks = !shared;
+    e->use_pdl = !shared;
     e->W = ((cfg->num_modes + 31) / 32);
     e->tr.cutoff_type = cfg->cutoff_type;
     e->tr.cutoff = cfg->cutoff;
@@ -1590,6 +1606,15 @@ mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const do
     if (s != MPX_OK) return bail(s);
     *out = e;
     return MPX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mpx_status mpx_create(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef, uint64_t n_obs,
+                      double core, const uint64_t *state_mask, mpx_engine **out) {
+    return create_engine(cfg, obs_words, obs_coef, n_obs, core, state_mask, out, false);
 }
 
 mpx_status mpx_propagate(mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n_layers) {
@@ -1949,13 +1974,10 @@ mpx_status mpx_trim_device_memory(int32_t device) {
     return MPX_OK;
 }
 
-// Internal (not exported): the batch runner's engines allocate straight from the pool and launch
-// without programmatic dependent launch (with several engines' streams sharing the GPU, a kernel
-// scheduled early would hold SM slots at its dependency wait that another engine's ready kernel needs).
-void mpx_internal_shared_gpu(mpx_engine *e, int32_t shared) {
-    if (e == nullptr) return;
-    e->keep_blocks = shared == 0;
-    e->use_pdl = shared == 0;
+// Internal (not exported): the batch runner's engines, created as sharing the GPU (see create_engine).
+mpx_status mpx_internal_create_shared(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef,
+                                      uint64_t n_obs, double core, const uint64_t *state_mask, mpx_engine **out) {
+    return create_engine(cfg, obs_words, obs_coef, n_obs, core, state_mask, out, true);
 }
 
 const char *mpx_last_error(const mpx_engine *e) { return e != nullptr ? e->err.c_str() : g_create_error.c_str(); }

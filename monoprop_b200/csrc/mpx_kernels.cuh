@@ -779,6 +779,53 @@ __global__ void k_build_table(Store st, Counters *__restrict__ cnt, uint64_t lo,
     }
 }
 
+// Store index of each of n query keys (kNoStall when absent): the open-addressing lookup of the resolve,
+// for host requests such as re-weighting the initial operator (MPOperator.h:193-232 finds each term of
+// the new operator in the store the same way).
+template <int W>
+__global__ void k_lookup(Store st, const uint64_t *__restrict__ qkeys, uint64_t nq, uint64_t n_live,
+                         uint32_t *__restrict__ out, Counters *__restrict__ cnt) {
+    for (uint64_t q = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; q < nq;
+         q += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t k[W];
+        load_key<W>(qkeys, q, k);
+        const uint64_t h = key_hash<W>(k);
+        const uint32_t tag = static_cast<uint32_t>(h >> 32);
+        uint64_t pos = h & st.tmask;
+        uint32_t found = kNoStall;
+        for (uint64_t probes = 0;; ++probes) {
+            if (probes > st.tmask) {
+                atomicOr(&cnt->err, 32u);
+                break;
+            }
+            const unsigned long long slot = st.table[pos];
+            if (slot == kEmptySlot) break;
+            const uint32_t idx = static_cast<uint32_t>(slot);
+            if (idx < n_live && static_cast<uint32_t>(slot >> 32) == tag) {
+                uint64_t o[W];
+                load_key<W>(st.keys, idx, o);
+                bool eq = true;
+#pragma unroll
+                for (int w = 0; w < W; ++w) eq = eq && (o[w] == k[w]);
+                if (eq) {
+                    found = idx;
+                    break;
+                }
+            }
+            pos = (pos + 1) & st.tmask;
+        }
+        out[q] = found;
+    }
+}
+
+// coef[idx[k]] = val[k] (indices distinct).
+__global__ void k_scatter(double *__restrict__ coef, const uint32_t *__restrict__ idx, const double *__restrict__ val,
+                          uint64_t n) {
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        coef[idx[k]] = val[k];
+}
+
 // <0|O|0>: per-block partial sums over contiguous chunks, fixed-order tree (MPOperator.h:235-254,
 // PauliAlgebra.h:144-147, MajoranaAlgebra.h:56-60).
 template <int W, int BASIS>

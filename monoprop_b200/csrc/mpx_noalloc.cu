@@ -83,14 +83,26 @@ __global__ void k_expect_chunked_final(const double *__restrict__ partial, uint3
     }
 }
 
-template <int W, int B>
-void launch(const uint64_t *keys, const double *coef, uint64_t n, const mpx::StateMask &sm, double *partial,
-            uint32_t blocks, cudaStream_t s) {
-    k_expect_chunked<W, B><<<blocks, mpx::kBlock, 0, s>>>(keys, coef, n, sm, partial);
+// Launches through cudaLaunchKernelEx, whose return value is the status of this launch alone: an error
+// left pending by the caller's earlier, unrelated work is neither reported as this call's failure nor
+// cleared.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_on(cudaStream_t s, uint32_t blocks, uint32_t threads, void (*kernel)(KArgs...), Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = s;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-using LaunchFn = void (*)(const uint64_t *, const double *, uint64_t, const mpx::StateMask &, double *, uint32_t,
-                          cudaStream_t);
+template <int W, int B>
+cudaError_t launch(const uint64_t *keys, const double *coef, uint64_t n, const mpx::StateMask &sm, double *partial,
+                   uint32_t blocks, cudaStream_t s) {
+    return launch_on(s, blocks, mpx::kBlock, &k_expect_chunked<W, B>, keys, coef, n, sm, partial);
+}
+
+using LaunchFn = cudaError_t (*)(const uint64_t *, const double *, uint64_t, const mpx::StateMask &, double *,
+                                 uint32_t, cudaStream_t);
 
 template <int W>
 LaunchFn pick_b(int basis) {
@@ -162,10 +174,13 @@ MPX_API mpx_status mpx_expectation_noalloc(int32_t basis, uint32_t words, const 
     for (uint32_t w = 0; w < words; ++w) sm.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
     const auto s = static_cast<cudaStream_t>(stream);
     const uint32_t blocks = static_cast<uint32_t>((n_terms + kNoAllocChunk - 1) / kNoAllocChunk);
-    if (blocks > 0) pick(static_cast<int>(words), basis)(keys, coefs, n_terms, sm, partial, blocks, s);
-    k_expect_chunked_final<<<1, 32, 0, s>>>(partial, blocks, core, out);
-    ce = cudaGetLastError();
-    if (ce != cudaSuccess) return nofail(MPX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(ce));
+    if (blocks > 0) {
+        ce = pick(static_cast<int>(words), basis)(keys, coefs, n_terms, sm, partial, blocks, s);
+        if (ce != cudaSuccess)
+            return nofail(MPX_ERR_CUDA, std::string("launch of the partial sums: ") + cudaGetErrorString(ce));
+    }
+    ce = launch_on(s, 1, 32, &k_expect_chunked_final, static_cast<const double *>(partial), blocks, core, out);
+    if (ce != cudaSuccess) return nofail(MPX_ERR_CUDA, std::string("launch of the final sum: ") + cudaGetErrorString(ce));
     return MPX_OK;
 }
 

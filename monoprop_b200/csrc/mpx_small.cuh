@@ -30,8 +30,12 @@ __host__ __device__ inline size_t small_smem_bytes(int W, uint32_t cap, uint32_t
            + static_cast<size_t>(cap / 32) * 4;            // leader-emitted bitmap
 }
 
+// Inserts term i into the shared table. The capacity keeps the load at or below 1/2, so a full table
+// means the store is inconsistent: the error flag is set (as the streaming kernels do) instead of
+// dropping the term silently.
 template <int W>
-__device__ __forceinline__ void small_insert(uint16_t *table, uint32_t tmask, const uint64_t *keys, uint32_t i) {
+__device__ __forceinline__ void small_insert(uint16_t *table, uint32_t tmask, const uint64_t *keys, uint32_t i,
+                                             Counters *__restrict__ cnt) {
     uint64_t k[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) k[w] = keys[i * W + w];
@@ -40,6 +44,7 @@ __device__ __forceinline__ void small_insert(uint16_t *table, uint32_t tmask, co
         if (atomicCAS(&table[pos], kSmallEmpty, static_cast<uint16_t>(i)) == kSmallEmpty) return;
         pos = (pos + 1) & tmask;
     }
+    atomicOr(&cnt->err, 16u);
 }
 
 template <int W, int BASIS>
@@ -69,7 +74,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
     for (uint32_t i = tid; i < n_in; i += kSmallThreads) coef[i] = st.coef[i];
     for (uint32_t i = tid; i <= tmask; i += kSmallThreads) table[i] = kSmallEmpty;
     __syncthreads();
-    for (uint32_t i = tid; i < n_in; i += kSmallThreads) small_insert<W>(table, tmask, keys, i);
+    for (uint32_t i = tid; i < n_in; i += kSmallThreads) small_insert<W>(table, tmask, keys, i, cnt);
     __syncthreads();
 
     for (uint32_t step = lo; step < hi; ++step) {
@@ -160,21 +165,29 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
             for (int w = 0; w < W; ++w) p[w] = keys[src * W + w] ^ gd.g[w];
             uint32_t pos = static_cast<uint32_t>(key_hash<W>(p)) & tmask;
             uint32_t found = kNoStall;
+            bool ended = false;
             for (uint32_t probes = 0; probes <= tmask; ++probes) {
                 const uint16_t t = table[pos];
-                if (t == kSmallEmpty) break;
+                if (t == kSmallEmpty) {
+                    ended = true;
+                    break;
+                }
                 if (t < n0) {
                     bool eq = true;
 #pragma unroll
                     for (int w = 0; w < W; ++w) eq = eq && keys[t * W + w] == p[w];
                     if (eq) {
                         found = t;
+                        ended = true;
                         break;
                     }
                 }
                 pos = (pos + 1) & tmask;
             }
-            if (found != kNoStall) {
+            if (!ended) { // every slot probed without an end: the table is inconsistent
+                atomicOr(&cnt->err, 16u);
+            }
+            else if (found != kNoStall) {
                 const bool leader_took_it = follower && ((emitb[found >> 5] >> (found & 31)) & 1u);
                 if (!leader_took_it) {
                     const double vt = coef[found] * inv_cos;
@@ -187,7 +200,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
 #pragma unroll
                 for (int w = 0; w < W; ++w) keys[idx * W + w] = p[w];
                 coef[idx] = (sinv * ph) * v;
-                small_insert<W>(table, tmask, keys, idx);
+                small_insert<W>(table, tmask, keys, idx, cnt);
             }
         }
         if (tid == 0) {

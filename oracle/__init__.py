@@ -29,16 +29,19 @@ PORT_LIB = os.path.join(HERE, "libmporacle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmpref.so")
 
 
-def build(reference_root: str = "/root/reference") -> None:
-    """Compile the C restatement, and the reference oracle when its sources are present."""
+def build(reference_root: str | None = None) -> None:
+    """Compile the C restatement, and the reference oracle when its sources are present.
+
+    ``reference_root`` (else ``$MONOPROP_REFERENCE``, else the default of ``oracle/build_ref.sh``) is the
+    reference source tree; without it the prebuilt ``oracle/_ref`` is kept as it is."""
     src = os.path.join(HERE, "mp_oracle.c")
     if not os.path.exists(PORT_LIB) or os.path.getmtime(src) > os.path.getmtime(PORT_LIB):
         # -ffp-contract=fast on an FMA target mirrors how the reference's own -O3 build contracts
         # c += s*phi*v into one fused multiply-add (checked bit-for-bit in tests/test_oracle.py).
         subprocess.check_call(["gcc", "-O2", "-march=x86-64-v3", "-ffp-contract=fast", "-shared", "-fPIC",
                                src, "-o", PORT_LIB, "-lm"])
-    if os.path.isdir(os.path.join(reference_root, "cpp", "monoprop")):
-        subprocess.check_call([os.path.join(HERE, "build_ref.sh"), reference_root])
+    reference_root = reference_root or os.environ.get("MONOPROP_REFERENCE")
+    subprocess.check_call([os.path.join(HERE, "build_ref.sh"), *([reference_root] if reference_root else [])])
 
 
 class _PortCfg(C.Structure):

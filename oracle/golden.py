@@ -8,6 +8,7 @@ import os
 import numpy as np
 
 from monoprop_b200.encoding import canonical_order, words_to_slots
+from monoprop_b200 import workloads as W
 from monoprop_b200.workloads import Workload
 
 GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden")
@@ -113,6 +114,102 @@ def check_against(g: dict, keys: np.ndarray, coefs: np.ndarray, ev: float, rtol:
         assert abs((c * c).sum() - float(g["coef_sumsq"])) <= rtol * max(1.0, float((c * c).sum()))
     e = float(g["expectation"])
     assert abs(ev - e) <= rtol * max(1.0, abs(e)), (ev, e)
+
+
+def _batch_instance(depth: int):
+    """The first instance of the 256-instance batched workload with ``depth`` layers."""
+    return next(wl for wl in W.batch_ising50(256) if wl.extra["depth"] == depth)
+
+
+#: full-depth workloads whose final stores are too large to keep in full (up to ~5e7 terms): only a
+#: bucketed digest is committed (``full_<name>.npz``). name -> zero-argument workload builder.
+FULL_DEPTH = {
+    "ising100": W.ising100,
+    "hubbard6x6": W.hubbard6x6,
+    "ising50_b24": lambda: _batch_instance(24),
+    "ising50_b12": lambda: _batch_instance(12),
+}
+
+DIGEST_BUCKETS = 2048
+DIGEST_TOP = 4096
+
+
+def _mix64(x: np.ndarray) -> np.ndarray:
+    """The splitmix64 finaliser on a uint64 array (wrapping arithmetic)."""
+    x = x.copy()
+    x ^= x >> np.uint64(30)
+    x *= np.uint64(0xBF58476D1CE4E5B9)
+    x ^= x >> np.uint64(27)
+    x *= np.uint64(0x94D049BB133111EB)
+    x ^= x >> np.uint64(31)
+    return x
+
+
+def key_hashes(keys: np.ndarray) -> np.ndarray:
+    """A 64-bit hash of every key row (``uint64[n, W]`` -> ``uint64[n]``)."""
+    h = np.zeros(keys.shape[0], dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        for w in range(keys.shape[1]):
+            h ^= _mix64(keys[:, w] + np.uint64(w))
+    return h
+
+
+def _unit(h: np.ndarray) -> np.ndarray:
+    """Pseudo-random weights in [-1, 1) from 64-bit hashes."""
+    return (h >> np.uint64(11)).astype(np.float64) * (2.0 ** -52) - 1.0
+
+
+def bucket_digest(keys: np.ndarray, coefs: np.ndarray, buckets: int = DIGEST_BUCKETS, top: int = DIGEST_TOP) -> dict:
+    """Size-independent digest of a raw store that still bounds every single coefficient.
+
+    Keys are sorted canonically; the key set is its SHA-256. Each key falls into one of ``buckets``
+    buckets by its hash and carries two pseudo-random weights w1, w2 in [-1, 1) from the hash; per
+    bucket the digest keeps the term count, sum |c|, sum c*w1 and sum c*w2 (summed in canonical key
+    order, so equal inputs give equal bits). If every coefficient agrees to ``rtol`` relative, every
+    projected sum agrees to ``rtol * sum |c|`` of its bucket; a single term off by more than that shows
+    up in both projections unless its weights vanish. The ``top`` largest coefficients are also kept
+    with their canonical positions, for a direct per-term comparison, and the SHA-256 of all coefficient
+    bits in key order records whether two stores are bit-identical."""
+    order = canonical_order(keys)
+    k, c = np.ascontiguousarray(keys[order]), np.ascontiguousarray(coefs[order])
+    h = key_hashes(k)
+    b = (h % np.uint64(buckets)).astype(np.int64)
+    with np.errstate(over="ignore"):
+        w1, w2 = _unit(h), _unit(_mix64(h ^ np.uint64(0x9E3779B97F4A7C15)))
+    a = np.abs(c)
+    t = min(top, c.shape[0])
+    pos = np.sort(np.argpartition(-a, t - 1)[:t]) if t > 0 else np.zeros(0, dtype=np.int64)
+    return {"n": np.int64(k.shape[0]), "sha256": np.bytes_(hashlib.sha256(k.tobytes()).hexdigest()),
+            "coef_sha256": np.bytes_(hashlib.sha256(c.tobytes()).hexdigest()),
+            "b_count": np.bincount(b, minlength=buckets).astype(np.int64),
+            "b_abs": np.bincount(b, weights=a, minlength=buckets),
+            "b_w1": np.bincount(b, weights=c * w1, minlength=buckets),
+            "b_w2": np.bincount(b, weights=c * w2, minlength=buckets),
+            "top_pos": pos.astype(np.int64), "top_keys": k[pos], "top_coefs": c[pos]}
+
+
+def check_digest(g: dict, keys: np.ndarray, coefs: np.ndarray, ev: float, rtol: float = 1e-10) -> bool:
+    """Asserts (keys, coefs, ev) against a :func:`bucket_digest` fixture: key set bit-exact, per-bucket
+    projections within ``rtol`` of the bucket's sum |c|, the largest coefficients within ``rtol`` relative,
+    <O> within ``rtol`` relative. Returns whether the coefficients are bit-identical to the fixture's."""
+    d = bucket_digest(keys, coefs, buckets=int(g["b_count"].shape[0]), top=0)
+    assert int(d["n"]) == int(g["n"]), (int(d["n"]), int(g["n"]))
+    assert d["sha256"].item() == g["sha256"].item(), "monomial set differs"
+    assert np.array_equal(d["b_count"], g["b_count"])
+    bound = rtol * np.maximum(d["b_abs"], g["b_abs"]) + 1e-300
+    for name in ("b_w1", "b_w2"):
+        err = np.abs(d[name] - g[name])
+        assert np.all(err <= bound), (name, float(np.max(err / bound)))
+    order = canonical_order(keys)
+    pos = g["top_pos"]
+    k = keys[order[pos]]
+    c = coefs[order[pos]]
+    assert np.array_equal(k, g["top_keys"])
+    tc = g["top_coefs"]
+    assert np.all(np.abs(c - tc) <= rtol * np.maximum(np.abs(c), np.abs(tc)) + 1e-300)
+    e = float(g["expectation"])
+    assert abs(ev - e) <= rtol * max(1.0, abs(e)), (ev, e)
+    return d["coef_sha256"].item() == g["coef_sha256"].item()
 
 
 def random_workload(seed: int, basis: str) -> Workload:

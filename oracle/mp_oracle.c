@@ -41,6 +41,7 @@
 #include <string.h>
 
 #define MPO_MAXW 8
+#define MPO_SCHRODINGER_MAX_TERMS (1ULL << 28) /* largest initial Schrodinger store the oracle builds */
 #define EVEN_MASK 0x5555555555555555ULL
 #define EMPTY_SLOT 0xFFFFFFFFu
 
@@ -284,6 +285,8 @@ static int phase_of(const mpo_state *s, const gate_ctx *c, const uint64_t *m, co
 
 /* --- public ABI ----------------------------------------------------------------------------------- */
 
+void mpo_destroy(void *hs);
+
 typedef struct {
     size_t src;
     uint64_t p[MPO_MAXW];
@@ -312,7 +315,10 @@ void *mpo_create(const mpo_config *cfg,
         s->n_obs = n_terms;
         s->obs_keys = malloc(sizeof(uint64_t) * W * (n_terms ? n_terms : 1));
         s->obs_coef = malloc(sizeof(double) * (n_terms ? n_terms : 1));
-        if (!s->obs_keys || !s->obs_coef) return NULL;
+        if (!s->obs_keys || !s->obs_coef) {
+            mpo_destroy(s);
+            return NULL;
+        }
         memcpy(s->obs_keys, words, sizeof(uint64_t) * W * n_terms);
         memcpy(s->obs_coef, coefs, sizeof(double) * n_terms);
         const int L = cfg->logical_modes;
@@ -320,12 +326,25 @@ void *mpo_create(const mpo_config *cfg,
         if (sc > 2 * L) sc = 2 * L;
         int K = sc / 2 + sc % 2;
         if (K > L) K = L;
+        /* the initial store holds sum_{k<=K} C(L, k) monomials: refuse sizes an oracle cannot hold */
+        double total = 0.0, binom = 1.0;
+        for (int k = 0; k <= K; ++k) {
+            total += binom;
+            binom = binom * (double)(L - k) / (double)(k + 1);
+        }
+        if (total > (double)MPO_SCHRODINGER_MAX_TERMS) {
+            mpo_destroy(s);
+            return NULL;
+        }
         int sel[256];
         for (int k = 0; k <= K; ++k) {
             /* subsets of k modes in lexicographic order */
             for (int i = 0; i < k; ++i) sel[i] = i;
             for (;;) {
-                if (reserve(s, s->n + 1) != 0) return NULL;
+                if (reserve(s, s->n + 1) != 0) {
+                    mpo_destroy(s);
+                    return NULL;
+                }
                 uint64_t *m = s->keys + s->n * W;
                 memset(m, 0, sizeof(uint64_t) * W);
                 for (int i = 0; i < k; ++i)
@@ -345,7 +364,10 @@ void *mpo_create(const mpo_config *cfg,
         }
         return s;
     }
-    if (reserve(s, n_terms ? n_terms : 1) != 0) return NULL;
+    if (reserve(s, n_terms ? n_terms : 1) != 0) {
+        mpo_destroy(s);
+        return NULL;
+    }
     for (size_t i = 0; i < n_terms; ++i) {
         memcpy(s->keys + s->n * W, words + i * W, sizeof(uint64_t) * W);
         s->coef[s->n] = coefs[i];

@@ -23,9 +23,16 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
   ``MajoranaOperator`` canonicalisation), with the fixture's exact energy and gradient and the reference
   engine's raw output at infinite cutoff (``cutoff = 2 n``).
 
-Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT] [--fd-full] [--len-k-only]`` (``--fd-full``
-adds the slow finite-difference golden of the full 100-qubit circuit; ``--len-k-only`` writes only the
-``only_rotate_len_k`` fixtures).
+* ``full_<workload>.npz`` -- the full-depth benchmark circuits (100-qubit kicked Ising, 5600 gates;
+  6x6 Hubbard, 2208 gates; two instances of the batched 50-qubit workload at depths 24 and 12), whose
+  final stores (up to ~4.4e7 terms) are kept as a bucketed digest (``oracle.golden.bucket_digest``): key
+  set SHA-256, per-bucket counts, sums of |c| and of two pseudo-random projections of c, the 4096 largest
+  coefficients with their positions, and <0|O|0>.
+
+Usage: ``python tests/golden/make_golden.py [REFERENCE_ROOT] [--fd-full] [--len-k-only] [--full-depth]``
+(``--fd-full`` adds the slow finite-difference golden of the full 100-qubit circuit; ``--len-k-only``
+writes only the ``only_rotate_len_k`` fixtures; ``--full-depth`` writes only the ``full_*`` digests, a few
+minutes on 8 cores). REFERENCE_ROOT defaults to ``$MONOPROP_REFERENCE``.
 """
 
 from __future__ import annotations
@@ -119,10 +126,28 @@ def fixture_workload(name: str, reference_root: str, lower_atol=None):
     return wl, float(d["actual_energy"]), np.asarray(d["actual_gradient"], dtype=np.float64)
 
 
-def main(reference_root: str = "/root/reference") -> None:
+def full_depth() -> None:
+    """Digests of the full-depth circuits, propagated by the reference with one partition (its raw
+    export needs the whole store in one partition)."""
+    for name, make in golden.FULL_DEPTH.items():
+        wl = make()
+        r = oracle.run_ref(wl)
+        d = golden.bucket_digest(r.keys, r.coefs)
+        np.savez_compressed(os.path.join(HERE, f"full_{name}.npz"), expectation=np.float64(r.expectation),
+                            n_layers=np.int64(wl.n_layers), seconds=np.float64(r.seconds), **d)
+        print("full", name, wl.n_layers, r.keys.shape[0], r.expectation, f"{r.seconds:.1f} s", flush=True)
+
+
+def main(reference_root: str | None = None) -> None:
+    reference_root = reference_root or os.environ.get("MONOPROP_REFERENCE")
+    if not reference_root:
+        raise SystemExit("give the reference source root as an argument or in $MONOPROP_REFERENCE")
     oracle.build(reference_root)
     if not oracle.ref_available():
         raise SystemExit("reference oracle could not be built")
+    if "--full-depth" in sys.argv:
+        full_depth()
+        return
     for name, make, L, k in LEN_K:
         wl = make()
         wl = dataclasses.replace(wl, extra={**wl.extra, "only_rotate_len_k": k})

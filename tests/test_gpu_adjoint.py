@@ -27,6 +27,12 @@ from oracle import golden
 
 pytestmark = pytest.mark.gpu
 
+# Per-angle finite-difference tolerance: |fd - grad| <= 1e-7 |fd| + FD_ATOL. FD_ATOL covers the central
+# difference's own error at h = 1e-5 (h^2 |f'''| / 6 + eps |<O>| / h, below 1e-10 for these circuits),
+# so an angle whose derivative is near zero is still held to an absolute 1e-9.
+FD_RTOL = 1e-7
+FD_ATOL = 1e-9
+
 
 def value_and_grad(wl, theta=None, segment_gates=0):
     dp = DifferentiablePropagation(wl, segment_gates=segment_gates)
@@ -84,13 +90,12 @@ def test_finite_differences_structural_truncation(make):
     ev, grad = value_and_grad(wl, theta)
     rng = np.random.default_rng(11)
     h = 1e-5
-    scale = np.max(np.abs(grad))
     for p in rng.choice(theta.size, size=min(64, theta.size), replace=False):
         tp, tm = theta.copy(), theta.copy()
         tp[p] += h
         tm[p] -= h
         fd = (expectation(wl, tp) - expectation(wl, tm)) / (2 * h)
-        assert abs(fd - grad[p]) <= 1e-7 * scale, (p, fd, grad[p])
+        assert abs(fd - grad[p]) <= FD_RTOL * abs(fd) + FD_ATOL, (p, fd, grad[p])
 
 
 def test_segments_and_final_state():
@@ -125,12 +130,13 @@ def test_torch_autograd():
 def test_full_circuit_gradient_finite_differences():
     """The 100-qubit, 5600-angle circuit with checkpoints every 4 circuit layers (1120 gates) against
     central finite differences (h = 1e-5) of the reference's replayed graph on 64 seeded angles
-    (tests/golden/fd_ising100.npz): 1e-7 relative to the largest derivative."""
+    (tests/golden/fd_ising100.npz): 1e-7 relative per angle."""
     g = golden.load("fd_ising100")
     ev, grad = value_and_grad(W.ising100(), segment_gates=4 * 280)
     assert abs(ev - float(g["expectation"])) <= 1e-10 * max(1.0, abs(float(g["expectation"])))
     fd = g["fd"]
-    assert np.max(np.abs(grad[g["idx"]] - fd)) <= 1e-7 * max(np.max(np.abs(fd)), np.max(np.abs(grad)))
+    err = np.abs(grad[g["idx"]] - fd)
+    assert np.all(err <= FD_RTOL * np.abs(fd) + FD_ATOL), (g["idx"][np.argmax(err)], float(np.max(err)))
 
 
 @pytest.mark.parametrize("make, L", [(W.hubbard6x6, 300), (W.ising100, 600)])

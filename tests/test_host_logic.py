@@ -53,6 +53,26 @@ def test_batch_run_rejects_null_buffers_without_touching_a_device():
     assert rc == 1 and b"NULL" in err.value
 
 
+def test_batch_run_rejects_a_device_it_cannot_use():
+    """An out-of-range device ordinal (or no device at all) is a non-OK status with a message, never a
+    silent MPX_OK with unwritten results."""
+    from monoprop_b200.batch import _Item, _Options
+
+    lib = _native.load()
+    cfg = _native.Config(1, 1, 4, 0, 0.0, 0, 0.0, 8, 999, 0, 0, 0)
+    ev = np.full(1, np.nan)
+    gw = np.zeros((1, 1), np.uint64)
+    an = np.zeros(1)
+    items = (_Item * 1)()
+    items[0].expectation, items[0].gen_words, items[0].angles, items[0].n_layers = (ev.ctypes.data, gw.ctypes.data,
+                                                                                   an.ctypes.data, 1)
+    opt = _Options(2, 0, 0)
+    err = C.create_string_buffer(256)
+    rc = lib.mpx_batch_run(C.byref(cfg), C.cast(items, C.c_void_p), 1, C.byref(opt), err, 256)
+    assert rc in (1, 6) and err.value  # MPX_ERR_INVALID (ordinal out of range) or MPX_ERR_NO_DEVICE
+    assert np.isnan(ev[0])
+
+
 def test_autotuner_sample_is_depth_stratified():
     batch = W.batch_ising50(40, seed=4)
     sample = Autotuner(cache_path="/nonexistent/x.json", sample=8).calibration_sample(batch)

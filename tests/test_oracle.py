@@ -45,6 +45,33 @@ def test_port_reproduces_reference_fixture(name):
         assert abs(r.expectation - float(g["exact_energy"])) <= 1e-12
 
 
+def test_port_matches_full_depth_hubbard_digest():
+    """The full 6x6 Hubbard circuit (2208 gates, 6.4e6 terms) against the reference's full-depth digest."""
+    wl = golden.FULL_DEPTH["hubbard6x6"]()
+    r = oracle.run_port(wl)
+    assert golden.check_digest(golden.load("full_hubbard6x6"), r.keys, r.coefs, r.expectation)
+
+
+def test_digest_detects_planted_errors():
+    """The bucketed digest catches one coefficient off by 1e-8 relative, one key changed, and one term
+    missing (mistakes planted in the oracle's own output)."""
+    r = oracle.run_port(W.line20())
+    g = golden.bucket_digest(r.keys, r.coefs)
+    g["expectation"] = np.float64(r.expectation)
+    assert golden.check_digest(g, r.keys, r.coefs, r.expectation)
+    i = int(np.argsort(np.abs(r.coefs))[r.coefs.size // 2])  # a mid-sized coefficient, not among the largest
+    bad = r.coefs.copy()
+    bad[i] *= 1 + 1e-8
+    with pytest.raises(AssertionError):
+        golden.check_digest(g, r.keys, bad, r.expectation)
+    keys = r.keys.copy()
+    keys[i, 0] ^= np.uint64(1)
+    with pytest.raises(AssertionError):
+        golden.check_digest(g, keys, r.coefs, r.expectation)
+    with pytest.raises(AssertionError):
+        golden.check_digest(g, r.keys[1:], r.coefs[1:], r.expectation)
+
+
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built here")
 @pytest.mark.parametrize("seed", range(12))
 @pytest.mark.parametrize("basis", ["pauli", "majorana"])

@@ -34,7 +34,9 @@ def _noalloc(lib, eng, basis_code, mask, core, out_ptr, stream):
     assert rc == 0, err.value.decode()
 
 
-@pytest.mark.parametrize("make, n_layers", [(W.line20, None), (W.hubbard6x6, 700)])
+# key widths 1 (20 qubits), 3 (72 modes), 2 (50 qubits) and 4 (100 qubits)
+@pytest.mark.parametrize("make, n_layers", [(W.line20, None), (W.hubbard6x6, 700), (lambda: W.ising50(3), None),
+                                            (W.ising100, 900)])
 def test_noalloc_expectation_matches_engine(make, n_layers):
     import torch
 
