@@ -115,6 +115,9 @@ MPX_API mpx_status mpx_reset(mpx_engine *e);
 
 /* Setters mirroring the reference properties (binder.h:154-185; MonomialPropagator.h:168-211). */
 MPX_API mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff);
+/* cutoff_type property setter (binder.h:176-184, update_cutoff_type): mpx_cutoff_type; Pauli engines accept
+ * only MPX_CUTOFF_SUPPORT (the reference's CutoffConfigError, a ValueError). */
+MPX_API mpx_status mpx_set_cutoff_type(mpx_engine *e, int32_t cutoff_type);
 MPX_API mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value);
 MPX_API mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value);
 
@@ -203,6 +206,16 @@ MPX_API mpx_status mpx_graph_expectation(mpx_engine *e, const mpx_circuit *c, do
 MPX_API mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation,
                                       double *grad_angles);
 
+/* Pares the stored graph of circuit c against the reference state (the pare_threshold of the reference's
+ * expectation_value[_and_gradient]_functional: pare_graph, PareGraph.cpp:103-141, keep set
+ * indices_above(threshold), MonomialPropagator.inl:950-960). Terms whose reference-state weight exceeds
+ * threshold are kept, and walking the layers backward so is every term whose value can still flow into a
+ * kept one; later mpx_graph_expectation / mpx_graph_gradient calls skip the cos scaling of every other
+ * term and the rotation of pairs with no kept endpoint. <0|O|0> and its gradient are unchanged for
+ * threshold in [0, 1) (fully paired terms have weight 1); the replayed coefficients of pared terms are not
+ * meaningful. threshold < 0 turns paring off. */
+MPX_API mpx_status mpx_graph_pare(mpx_engine *e, const mpx_circuit *c, double threshold);
+
 /* Pair log of a gradient forward pass (mpx_adjoint_forward, mpx_graph_build). The forward pass records
  * every gate's rotated and appended pairs (source, partner, phase), so that mpx_adjoint_backward replays
  * its segments without the hash resolve and mpx_graph_build needs no second pass; if the log overflows,
@@ -226,6 +239,42 @@ MPX_API mpx_status mpx_kernel_times(mpx_engine *e, double *sweep_ms, double *res
  * each time). This hands the kept blocks back to the pool and returns the pool's unused memory to the
  * driver. No reference counterpart (the reference is host-only). */
 MPX_API mpx_status mpx_trim_device_memory(int32_t device);
+
+/* Re-weights the initial operator. Replaces MonomialPropagator<N>::update_initial_operator (binder.h:153-156;
+ * MonomialPropagator.h:277, MPOperator.h:193-232, Heisenberg branch): every key of words [n][W] must
+ * already be in the store (the reference raises OperatorTermNotFound, a RuntimeError, otherwise: here
+ * MPX_ERR_STATE with *missing = the index of the first absent key); the current coefficients become coefs
+ * at those keys and zero elsewhere, and graph evaluations (mpx_graph_expectation / _gradient) start from
+ * this operator until the next mpx_reset or mpx_graph_build. has_core: core replaces the empty-monomial
+ * coefficient. */
+MPX_API mpx_status mpx_update_initial_operator(mpx_engine *e, const uint64_t *words, const double *coefs, uint64_t n,
+                                               int32_t has_core, double core, uint64_t *missing);
+
+/* Device memory the engine holds, by part. Replaces the accounting behind the reference's
+ * operator_memory_bytes / operator_memory_breakdown / graph_memory_bytes (binder.h:252-273,
+ * MonomialPropagator.h:124-135): keys and coefficients at the store's capacity, the hash table, the
+ * bit-column anticommutation index (the reference's InvertedIndex), per-gate scratch, the initial
+ * operator, and the frozen graph (pairs and per-step arrays). */
+typedef struct {
+    uint64_t terms, capacity;
+    uint32_t words;
+    uint64_t key_bytes, coef_bytes, table_bytes, column_bytes, scratch_bytes, initial_bytes;
+    uint64_t graph_layers, graph_pairs, graph_bytes;
+} mpx_memory_info;
+MPX_API mpx_status mpx_memory(mpx_engine *e, mpx_memory_info *out);
+
+/* Frozen graph sizes. Replaces MonomialPropagator<N>::graph_size (MonomialPropagator.h:103-104):
+ * *pairs = rotated and appended pairs over all layers (the reference's cycles), *cos_only = anticommuting
+ * terms outside every pair (only cos-scaled), *layers = graph layers. All zero without a graph. */
+MPX_API mpx_status mpx_graph_info(mpx_engine *e, uint64_t *layers, uint64_t *pairs, uint64_t *cos_only);
+
+/* Deep copy of an engine: store, settings, re-weighted initial operator and frozen graph; with c (the
+ * circuit of e's graph, or any circuit of e) also a copy of that circuit for the clone (*c_out). Replaces
+ * the reference's __deepcopy__ (binder.h:113-116), which clones the operator store and shares the graph. */
+MPX_API mpx_status mpx_clone(mpx_engine *e, const mpx_circuit *c, mpx_engine **out, mpx_circuit **c_out);
+
+/* The calling thread's current CUDA device (the default device of new engines in the Python module). */
+MPX_API mpx_status mpx_current_device(int32_t *device);
 
 MPX_API const char *mpx_last_error(const mpx_engine *e);
 

@@ -26,7 +26,8 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_stream", "mpx_launch_count", "mpx_adjoint_forward", "mpx_adjoint_backward", "mpx_graph_build", "mpx_graph_expectation",
             "mpx_graph_gradient", "mpx_set_pair_log", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
-            "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run")
+            "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run", "mpx_update_initial_operator", "mpx_memory",
+            "mpx_graph_info", "mpx_clone", "mpx_current_device", "mpx_graph_pare", "mpx_set_cutoff_type")
 
 
 class MpxError(RuntimeError):
@@ -46,6 +47,15 @@ class Config(C.Structure):
                 ("has_lower_atol", C.c_int32), ("lower_atol", C.c_double), ("has_upper_atol", C.c_int32),
                 ("upper_atol", C.c_double), ("num_modes", C.c_int32), ("device", C.c_int32),
                 ("capacity_hint", C.c_uint64), ("blocks_per_sm", C.c_int32), ("table_shift", C.c_int32)]
+
+
+class MemoryInfo(C.Structure):
+    """``mpx_memory_info``: device bytes the engine holds, by part."""
+
+    _fields_ = [("terms", C.c_uint64), ("capacity", C.c_uint64), ("words", C.c_uint32), ("key_bytes", C.c_uint64),
+                ("coef_bytes", C.c_uint64), ("table_bytes", C.c_uint64), ("column_bytes", C.c_uint64),
+                ("scratch_bytes", C.c_uint64), ("initial_bytes", C.c_uint64), ("graph_layers", C.c_uint64),
+                ("graph_pairs", C.c_uint64), ("graph_bytes", C.c_uint64)]
 
 
 _lib = None
@@ -96,6 +106,13 @@ def load() -> C.CDLL:
             "mpx_expectation_noalloc": (st, [C.c_int32, C.c_uint32, vp, vp, u64, vp, C.c_double, vp, vp, C.c_char_p,
                                              C.c_size_t]),
             "mpx_batch_run": (st, [C.POINTER(Config), vp, u64, vp, C.c_char_p, C.c_size_t]),
+            "mpx_update_initial_operator": (st, [vp, vp, vp, u64, C.c_int32, C.c_double, C.POINTER(u64)]),
+            "mpx_memory": (st, [vp, C.POINTER(MemoryInfo)]),
+            "mpx_graph_info": (st, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)]),
+            "mpx_clone": (st, [vp, vp, C.POINTER(vp), C.POINTER(vp)]),
+            "mpx_current_device": (st, [C.POINTER(C.c_int32)]),
+            "mpx_graph_pare": (st, [vp, vp, C.c_double]),
+            "mpx_set_cutoff_type": (st, [vp, C.c_int32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)

@@ -245,7 +245,53 @@ struct Frozen {
     const int8_t *code;                  // phase (+1 / -1 / 0) | 0x10 for an appended partner
     const uint64_t *p_begin;             // [n_steps] first pair of each step
     const unsigned long long *p_count;   // [n_steps] pairs of each step
+    // Paring (PareGraph.cpp:103-141): last[i] = the last step after which term i can still reach <0|O|0>
+    // (-1: never); a step skips the cos scaling of a term with last < step and the rotation of a pair with
+    // both endpoints below it. nullptr: no paring.
+    const int32_t *last;
 };
+
+// ----- paring ---------------------------------------------------------------------------------------------
+//
+// The reference pares a graph against the reference state (pare_graph, PareGraph.cpp:103-141, keep set
+// state.indices_above(threshold), MonomialPropagator.inl:950-960): walking the layers backward, a term is
+// kept while its value can still flow into a kept term, and the cos scaling of every other term is skipped.
+// The value of <0|O|0> (and its gradient) is unchanged: only terms that can never reach a scored term lose
+// their scaling. Relevance only grows toward earlier steps (a pair with one relevant endpoint makes both
+// relevant before the gate; a cos-only term keeps its status), so one int per term says up to which step
+// the term matters.
+
+// last[i] = n_steps - 1 where term i's reference-state weight exceeds the threshold (|weight| = 1 on a fully
+// paired term, 0 elsewhere: indices_above, MPFunctions.cpp:96-105), else -1.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_pare_init(const uint64_t *__restrict__ keys, uint64_t n, int32_t keep_paired,
+                                                       int32_t last_step, int32_t *__restrict__ last) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t m[W];
+        load_key<W>(keys, i, m);
+        uint64_t unpaired = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) unpaired |= (m[w] & kEven) ^ ((m[w] >> 1) & kEven);
+        last[i] = (unpaired == 0 && keep_paired) ? last_step : -1;
+    }
+}
+
+// One step, backward: a pair with an endpoint still relevant after the step makes both endpoints relevant
+// before it. The pairs of one step are disjoint, so no two threads touch the same term.
+__global__ void __launch_bounds__(kBlock) k_pare_step(Frozen fz, uint32_t step, int32_t *__restrict__ last) {
+    const uint64_t b = fz.p_begin[step], cnt = fz.p_count[step];
+    const int32_t st = static_cast<int32_t>(step);
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < cnt;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t s = fz.src[b + k], t = fz.tgt[b + k];
+        const int32_t ls = last[s], lt = last[t];
+        if (ls >= st || lt >= st) {
+            if (ls < st - 1) last[s] = st - 1;
+            if (lt < st - 1) last[t] = st - 1;
+        }
+    }
+}
 
 // Pairs of one frozen gate; with LOG also their pre-gate values into the tape's pair log (the slot of
 // pair k is p_base[step] + k, so no counters are needed).
@@ -265,8 +311,12 @@ __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ co
         const bool appended = (code & 0x10) != 0;
         const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
         const double vs = coef[s], vt = appended ? 0.0 : coef[t];
-        coef[s] = C * vs - S * phi * vt;
-        coef[t] = C * vt + S * phi * vs;
+        const bool pared = fz.last != nullptr && fz.last[s] < static_cast<int32_t>(step) &&
+                           fz.last[t] < static_cast<int32_t>(step);
+        if (!pared) {
+            coef[s] = C * vs - S * phi * vt;
+            coef[t] = C * vt + S * phi * vs;
+        }
         atomicOr(&done[s >> 5], 1u << (s & 31));
         if (!appended) atomicOr(&done[t >> 5], 1u << (t & 31));
         if constexpr (LOG) {

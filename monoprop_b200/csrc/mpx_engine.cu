@@ -38,6 +38,7 @@ struct mpx_circuit {
     bool persistent = false; // uploaded by mpx_circuit_upload (worth a CUDA graph)
     uint64_t n = 0;
     std::vector<uint64_t> words; // host copy of the generators, for mpx_circuit_set_angles
+    std::vector<double> angles;  // host copy of the current angles (a cloned engine re-uploads the circuit)
     int W = 1;
     int device = 0;
     bool any_cos_zero = false; // some gate has cos(2 angle) == 0 exactly (needs the pre-gate copy `aux`)
@@ -76,6 +77,11 @@ struct FrozenGraph {
     std::vector<uint64_t> n0, anti, count;  // per step (host)
     uint32_t *w_anti = nullptr;             // [L][sweep warps] anticommuting terms per sweep warp (build)
     uint32_t *done = nullptr;               // [ceil(n_final / 32)] scratch bitmap
+    int32_t *last = nullptr;                // paring (mpx_graph_pare): [n_final] last relevant step per term
+    bool pared = false;                     // the frozen kernels skip pared terms
+    double last_for = -1.0;                 // threshold `last` was computed for (< 0: none yet)
+    // the device view the frozen kernels take
+    Frozen view() const { return Frozen{src, tgt, code, p_begin, p_count, pared ? last : nullptr}; }
 };
 
 struct mpx_engine {
@@ -130,6 +136,12 @@ struct mpx_engine {
     uint64_t rec_hint = 0; // pair records the last recording forward pass needed (sizes the next log)
     int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity
     uint64_t *d_basis = nullptr; // basis_change rows [2T][W] (tr.basis_rows points here when set)
+    // Re-weighted initial operator (mpx_update_initial_operator): store indices and coefficients that
+    // graph evaluations start from instead of the constructor's operator.
+    uint32_t *d_start_idx = nullptr;
+    double *d_start_val = nullptr;
+    uint64_t n_start = 0;
+    bool start_on = false;
     // Large blocks through the kept-block cache (dev_alloc). The batch runner turns it off for its
     // engines: with several engines growing at once, power-of-two classes and idle kept blocks crowd
     // the device, and a 96-instance gradient batch took 2x longer with them.
@@ -453,7 +465,7 @@ template <int W, bool LOG>
 void launch_frozen(mpx_engine *e, const GateDesc *d_desc, const Frozen &fz, uint32_t gate, uint32_t step, uint64_t n0,
                    uint32_t *done, const Tape &tp) {
     launch_dep(e, &k_frozen_pairs<LOG>, e->st.coef, fz, d_desc, gate, step, done, tp);
-    launch_dep(e, &k_frozen_scan<W, LOG>, e->st, d_desc, gate, step, n0, done, tp);
+    launch_dep(e, &k_frozen_scan<W, LOG>, e->st, d_desc, gate, step, n0, done, tp, fz.last);
 }
 
 using FrozenFn = void (*)(mpx_engine *, const GateDesc *, const Frozen &, uint32_t, uint32_t, uint64_t, uint32_t *,
@@ -571,6 +583,26 @@ AdjInitFn pick_adj_init(int W, int basis) {
     default: return adj_init_fn<8>(basis);
     }
 }
+template <int W>
+void launch_lookup(mpx_engine *e, const uint64_t *qkeys, uint64_t nq, uint64_t n_live, uint32_t *out) {
+    const uint64_t blocks = std::min<uint64_t>((nq + 255) / 256, 4096);
+    k_lookup<W><<<static_cast<unsigned>(std::max<uint64_t>(blocks, 1)), 256, 0, e->stream>>>(e->st, qkeys, nq, n_live,
+                                                                                          out, e->d_cnt);
+}
+using LookupFn = void (*)(mpx_engine *, const uint64_t *, uint64_t, uint64_t, uint32_t *);
+LookupFn pick_lookup(int W) {
+    switch (W) {
+    case 1: return &launch_lookup<1>;
+    case 2: return &launch_lookup<2>;
+    case 3: return &launch_lookup<3>;
+    case 4: return &launch_lookup<4>;
+    case 5: return &launch_lookup<5>;
+    case 6: return &launch_lookup<6>;
+    case 7: return &launch_lookup<7>;
+    default: return &launch_lookup<8>;
+    }
+}
+
 BuildFn pick_table(int W) {
     switch (W) {
     case 1: return &launch_table<1>;
@@ -791,6 +823,7 @@ mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const doub
     for (const GateDesc &g : h) cd.any_cos_zero = cd.any_cos_zero || g.cos_zero;
     cd.device = e->device;
     cd.words.assign(gen_words, gen_words + n * e->W);
+    cd.angles.assign(angles, angles + n);
     return MPX_OK;
 }
 
@@ -1199,7 +1232,7 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
     const FrozenFn frozen_replay = pick_frozen<true>(e->W);
     Frozen fz{};
-    if (fg != nullptr) fz = Frozen{fg->src, fg->tgt, fg->code, fg->p_begin, fg->p_count};
+    if (fg != nullptr) fz = fg->view();
     for (size_t sg = S; sg-- > 0;) {
         const uint64_t lo = A.seg_lo[sg], hi = sg + 1 < S ? A.seg_lo[sg + 1] : L;
         const uint64_t n = A.ck_n[sg];
@@ -1289,16 +1322,82 @@ void free_graph(mpx_engine *e) {
     FrozenGraph &g = e->fg;
     for (void *p : {static_cast<void *>(g.src), static_cast<void *>(g.tgt), static_cast<void *>(g.code),
                     static_cast<void *>(g.p_begin), static_cast<void *>(g.p_count), static_cast<void *>(g.w_anti),
-                    static_cast<void *>(g.done)})
+                    static_cast<void *>(g.done), static_cast<void *>(g.last)})
         dev_free(e, p);
     g = FrozenGraph{};
 }
 
+template <int W>
+void launch_pare_init(mpx_engine *e, uint64_t n, int32_t keep_paired, int32_t last_step, int32_t *last) {
+    const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock, static_cast<uint64_t>(e->grid) * 4);
+    k_pare_init<W><<<static_cast<unsigned>(std::max<uint64_t>(blocks, 1)), kBlock, 0, e->stream>>>(e->st.keys, n,
+                                                                                                 keep_paired, last_step,
+                                                                                                 last);
+}
+using PareInitFn = void (*)(mpx_engine *, uint64_t, int32_t, int32_t, int32_t *);
+PareInitFn pick_pare_init(int W) {
+    switch (W) {
+    case 1: return &launch_pare_init<1>;
+    case 2: return &launch_pare_init<2>;
+    case 3: return &launch_pare_init<3>;
+    case 4: return &launch_pare_init<4>;
+    case 5: return &launch_pare_init<5>;
+    case 6: return &launch_pare_init<6>;
+    case 7: return &launch_pare_init<7>;
+    default: return &launch_pare_init<8>;
+    }
+}
+
+// Pares the frozen graph against the reference state at `threshold` (the reference's pare_graph,
+// PareGraph.cpp:103-141): last[i] from the scored terms, then one backward step per layer over its pairs.
+mpx_status graph_pare(mpx_engine *eng, double threshold) {
+    mpx_engine *e = eng;
+    FrozenGraph &g = e->fg;
+    if (threshold < 0.0) { // a negative threshold keeps every term (indices_above): no paring
+        g.pared = false;
+        return MPX_OK;
+    }
+    if (g.last != nullptr && g.last_for == threshold) {
+        g.pared = true;
+        return MPX_OK;
+    }
+    if (g.last == nullptr)
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&g.last), std::max<uint64_t>(g.n_final, 1) * sizeof(int32_t)));
+    // |weight| = 1 on fully paired terms: kept iff 1 > threshold
+    pick_pare_init(e->W)(e, g.n_final, 1.0 > threshold ? 1 : 0, static_cast<int32_t>(g.L) - 1, g.last);
+    const Frozen fz = Frozen{g.src, g.tgt, g.code, g.p_begin, g.p_count, nullptr};
+    for (uint64_t st = g.L; st-- > 0;) {
+        const uint64_t cnt = g.count[st];
+        if (cnt == 0) continue;
+        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((cnt + kBlock - 1) / kBlock,
+                                                                         static_cast<uint64_t>(e->grid)));
+        k_pare_step<<<blocks, kBlock, 0, e->stream>>>(fz, static_cast<uint32_t>(st), g.last);
+        ++e->launches;
+    }
+    MPX_CUDA(cudaGetLastError());
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    g.pared = true;
+    g.last_for = threshold;
+    return MPX_OK;
+}
+
 // Build: the gradient forward pass (checkpoints, per-warp counts), then every segment replayed once with
 // the streaming kernels to collect each gate's pairs into the graph.
+// Drops a re-weighted initial operator (mpx_update_initial_operator): reset and graph builds start from
+// the constructor's operator again.
+void clear_start(mpx_engine *e) {
+    dev_free(e, e->d_start_idx);
+    dev_free(e, e->d_start_val);
+    e->d_start_idx = nullptr;
+    e->d_start_val = nullptr;
+    e->n_start = 0;
+    e->start_on = false;
+}
+
 mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
     mpx_engine *e = eng;
     free_graph(e);
+    clear_start(e);
     mpx_status s = adjoint_forward(e, cd, segment_gates);
     if (s != MPX_OK) return s;
     AdjointState &A = e->adj;
@@ -1444,13 +1543,22 @@ mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segmen
     FrozenGraph &g = e->fg;
     const uint64_t L = g.L, nf = g.n_final;
     free_adjoint(e);
-    if (e->n_init > 0)
-        MPX_CUDA(cudaMemcpyAsync(e->st.coef, e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToDevice,
-                                 e->stream));
-    if (nf > e->n_init)
-        MPX_CUDA(cudaMemsetAsync(e->st.coef + e->n_init, 0, (nf - e->n_init) * sizeof(double), e->stream));
+    if (e->start_on) {
+        // the re-weighted initial operator (mpx_update_initial_operator), in store positions
+        if (nf > 0) MPX_CUDA(cudaMemsetAsync(e->st.coef, 0, nf * sizeof(double), e->stream));
+        if (e->n_start > 0)
+            k_scatter<<<static_cast<unsigned>(std::min<uint64_t>((e->n_start + 255) / 256, 4096)), 256, 0, e->stream>>>(
+                e->st.coef, e->d_start_idx, e->d_start_val, e->n_start);
+    }
+    else {
+        if (e->n_init > 0)
+            MPX_CUDA(cudaMemcpyAsync(e->st.coef, e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     e->stream));
+        if (nf > e->n_init)
+            MPX_CUDA(cudaMemsetAsync(e->st.coef + e->n_init, 0, (nf - e->n_init) * sizeof(double), e->stream));
+    }
     MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
-    const Frozen fz{g.src, g.tgt, g.code, g.p_begin, g.p_count};
+    const Frozen fz = g.view();
     const FrozenFn run = pick_frozen<false>(e->W);
     const uint64_t K = segment_gates == 0 ? std::max<uint64_t>(L, 1) : segment_gates;
     for (uint64_t st = 0; st < L; ++st) {
@@ -1660,6 +1768,7 @@ mpx_status mpx_circuit_set_angles(mpx_engine *e, mpx_circuit *c, const double *a
     for (uint64_t l = 0; l < c->n; ++l) make_desc(e, c->words.data() + l * e->W, angles[l], h[l]);
     c->any_cos_zero = false;
     for (const GateDesc &g : h) c->any_cos_zero = c->any_cos_zero || g.cos_zero;
+    c->angles.assign(angles, angles + c->n);
     MPX_CUDA(cudaSetDevice(e->device));
     if (c->n > 0) {
         MPX_CUDA(cudaMemcpyAsync(c->d_desc, h.data(), c->n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));
@@ -1760,6 +1869,7 @@ mpx_status mpx_reset(mpx_engine *e) {
     mpx_engine *eng = e;
     MPX_CUDA(cudaSetDevice(e->device));
     free_adjoint(e);
+    clear_start(e);
     return load_initial(e);
 }
 
@@ -1768,6 +1878,20 @@ mpx_status mpx_set_cutoff(mpx_engine *e, uint32_t cutoff) {
     clear_graphs(e); // truncation settings are kernel arguments baked into captured graphs
     e->cfg.cutoff = cutoff;
     e->tr.cutoff = cutoff;
+    return MPX_OK;
+}
+
+mpx_status mpx_set_cutoff_type(mpx_engine *e, int32_t cutoff_type) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    if (cutoff_type != MPX_CUTOFF_LENGTH && cutoff_type != MPX_CUTOFF_SUPPORT)
+        return fail(e, MPX_ERR_INVALID, "cutoff_type must be 'length' or 'support'");
+    if (e->cfg.basis == MPX_BASIS_PAULI && cutoff_type != MPX_CUTOFF_SUPPORT)
+        return fail(e, MPX_ERR_INVALID,
+                    "Pauli basis requires cutoff_type == Support (Length has no Pauli-weight meaning under the "
+                    "Pauli encoding).");
+    clear_graphs(e); // truncation settings are kernel arguments baked into captured graphs
+    e->cfg.cutoff_type = cutoff_type;
+    e->tr.cutoff_type = cutoff_type;
     return MPX_OK;
 }
 
@@ -1931,6 +2055,15 @@ mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segm
     return s;
 }
 
+mpx_status mpx_graph_pare(mpx_engine *e, const mpx_circuit *c, double threshold) {
+    if (e == nullptr || c == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    mpx_status s = check_graph(e, c);
+    if (s != MPX_OK) return s;
+    MPX_CUDA(cudaSetDevice(e->device));
+    return graph_pare(e, threshold);
+}
+
 mpx_status mpx_set_pair_log(mpx_engine *e, int64_t capacity) {
     if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
     e->pair_log = capacity;
@@ -1974,6 +2107,265 @@ mpx_status mpx_trim_device_memory(int32_t device) {
     return MPX_OK;
 }
 
+mpx_status mpx_update_initial_operator(mpx_engine *e, const uint64_t *words, const double *coefs, uint64_t n,
+                                       int32_t has_core, double core, uint64_t *missing) {
+    if (e == nullptr || (n > 0 && (words == nullptr || coefs == nullptr))) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    MPX_CUDA(cudaSetDevice(e->device));
+    uint64_t n_live = 0;
+    mpx_status s = mpx_size(e, &n_live);
+    if (s != MPX_OK) return s;
+    uint64_t *d_keys = nullptr;
+    uint32_t *d_idx = nullptr;
+    double *d_val = nullptr;
+    std::vector<uint32_t> idx(n);
+    cudaError_t ce = dev_alloc(e, reinterpret_cast<void **>(&d_keys), std::max<uint64_t>(n, 1) * e->W * sizeof(uint64_t));
+    if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&d_idx), std::max<uint64_t>(n, 1) * sizeof(uint32_t));
+    if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&d_val), std::max<uint64_t>(n, 1) * sizeof(double));
+    if (ce == cudaSuccess && n > 0) {
+        ce = cudaMemcpyAsync(d_keys, words, n * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(d_val, coefs, n * sizeof(double), cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess) {
+            pick_lookup(e->W)(e, d_keys, n, n_live, d_idx);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(idx.data(), d_idx, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    }
+    auto drop = [&]() {
+        dev_free(e, d_keys);
+        dev_free(e, d_idx);
+        dev_free(e, d_val);
+    };
+    if (ce != cudaSuccess) {
+        drop();
+        cudaGetLastError();
+        return fail(eng, ce == cudaErrorMemoryAllocation ? MPX_ERR_NOMEM : MPX_ERR_CUDA,
+                    std::string("initial operator update: ") + cudaGetErrorString(ce));
+    }
+    if (n > 0 && e->h_cnt->err != 0) {
+        drop();
+        return fail(eng, MPX_ERR_STATE, "hash table probe limit reached (internal error); the store is invalid");
+    }
+    for (uint64_t k = 0; k < n; ++k) {
+        if (idx[k] == kNoStall) {
+            drop();
+            if (missing != nullptr) *missing = k;
+            return fail(eng, MPX_ERR_STATE, "Operator term not found in the operator.");
+        }
+    }
+    // the current coefficients become the new operator (zero elsewhere); graph evaluations start from it
+    if (n_live > 0) MPX_CUDA(cudaMemsetAsync(e->st.coef, 0, n_live * sizeof(double), e->stream));
+    if (n > 0)
+        k_scatter<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 4096)), 256, 0, e->stream>>>(e->st.coef, d_idx,
+                                                                                                       d_val, n);
+    e->launches += n > 0 ? 2 : 0;
+    MPX_CUDA(cudaGetLastError());
+    dev_free(e, d_keys);
+    dev_free(e, e->d_start_idx);
+    dev_free(e, e->d_start_val);
+    e->d_start_idx = d_idx;
+    e->d_start_val = d_val;
+    e->n_start = n;
+    e->start_on = true;
+    if (has_core) e->core = core;
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    return MPX_OK;
+}
+
+mpx_status mpx_memory(mpx_engine *e, mpx_memory_info *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    uint64_t n = 0;
+    mpx_status s = mpx_size(e, &n);
+    if (s != MPX_OK) return s;
+    const uint64_t W = static_cast<uint64_t>(e->W);
+    *out = mpx_memory_info{};
+    out->terms = n;
+    out->capacity = e->st.cap;
+    out->words = static_cast<uint32_t>(W);
+    out->key_bytes = e->st.cap * W * sizeof(uint64_t);
+    out->coef_bytes = e->st.cap * sizeof(double);
+    out->table_bytes = (e->st.tmask + 1) * sizeof(unsigned long long);
+    out->column_bytes = (64 * W + 1) * e->st.cstride * sizeof(uint32_t);
+    out->scratch_bytes = e->sc.q_cap * (sizeof(uint32_t) + sizeof(uint8_t) + sizeof(double)) +
+                         e->st.cstride * sizeof(uint32_t) + (e->aux_on ? e->st.cap * sizeof(double) : 0);
+    out->initial_bytes = e->n_init * (W * sizeof(uint64_t) + sizeof(double)) +
+                         e->n_start * (sizeof(uint32_t) + sizeof(double));
+    const FrozenGraph &g = e->fg;
+    uint64_t pairs = 0;
+    for (uint64_t c : g.count) pairs += c;
+    out->graph_layers = g.L;
+    out->graph_pairs = pairs;
+    out->graph_bytes = g.L == 0 ? 0
+                                : pairs * (2 * sizeof(uint32_t) + sizeof(int8_t)) +
+                                      g.L * (sizeof(uint64_t) + sizeof(unsigned long long)) +
+                                      g.L * static_cast<uint64_t>(e->grid) * kWarps * sizeof(uint32_t) +
+                                      ((g.n_final + 31) / 32) * sizeof(uint32_t);
+    return MPX_OK;
+}
+
+mpx_status mpx_graph_info(mpx_engine *e, uint64_t *layers, uint64_t *pairs, uint64_t *cos_only) {
+    if (e == nullptr) return fail(nullptr, MPX_ERR_INVALID, "engine is NULL");
+    const FrozenGraph &g = e->fg;
+    uint64_t p = 0, c = 0;
+    for (uint64_t st = 0; st < g.L; ++st) {
+        const uint64_t appended = (st + 1 < g.L ? g.n0[st + 1] : g.n_final) - g.n0[st];
+        p += g.count[st];
+        // anticommuting terms outside every pair: a pair covers its emitter and, unless the partner was
+        // appended by this gate, its partner
+        c += g.anti[st] + appended - 2 * g.count[st];
+    }
+    if (layers) *layers = g.L;
+    if (pairs) *pairs = p;
+    if (cos_only) *cos_only = c;
+    return MPX_OK;
+}
+
+namespace {
+
+// Copies e's store, settings, last per-gate counters, re-weighted initial operator and frozen graph into
+// the freshly created engine d (same configuration, so the same capacities and strides).
+mpx_status clone_into(mpx_engine *e, mpx_engine *d) {
+    mpx_engine *eng = d;
+    const int W = e->W;
+    d->tr = e->tr;
+    d->tr.basis_rows = nullptr;
+    d->pair_log = e->pair_log;
+    d->rec_hint = e->rec_hint;
+    d->small_path = e->small_path;
+    d->use_graphs = e->use_graphs;
+    if (e->d_basis != nullptr) {
+        const size_t bytes = static_cast<size_t>(64 * W) * W * sizeof(uint64_t);
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&d->d_basis), bytes));
+        MPX_CUDA(cudaMemcpyAsync(d->d_basis, e->d_basis, bytes, cudaMemcpyDeviceToDevice, d->stream));
+        if (e->tr.basis_rows != nullptr) d->tr.basis_rows = d->d_basis;
+    }
+    d->aux_on = e->aux_on;
+    mpx_status s = alloc_store(d, e->st.cap, 0);
+    if (s != MPX_OK) return s;
+    uint64_t n = 0;
+    s = mpx_size(e, &n);
+    if (s != MPX_OK) return s;
+    if (n > 0) {
+        MPX_CUDA(cudaMemcpyAsync(d->st.keys, e->st.keys, n * W * sizeof(uint64_t), cudaMemcpyDeviceToDevice, d->stream));
+        MPX_CUDA(cudaMemcpyAsync(d->st.coef, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, d->stream));
+    }
+    MPX_CUDA(cudaMemcpyAsync(d->st.cols, e->st.cols, (64 * W + 1) * e->st.cstride * sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, d->stream));
+    MPX_CUDA(cudaMemcpyAsync(d->st.table, e->st.table, (e->st.tmask + 1) * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToDevice, d->stream));
+    MPX_CUDA(cudaMemcpyAsync(d->d_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToDevice, d->stream));
+    if (e->last_gates > 0) {
+        s = ensure_stats(d, e->last_gates);
+        if (s != MPX_OK) return s;
+        MPX_CUDA(cudaMemcpyAsync(d->d_stats, e->d_stats, 4 * e->last_gates * sizeof(uint64_t), cudaMemcpyDeviceToDevice,
+                                 d->stream));
+        d->last_gates = e->last_gates;
+    }
+    if (e->start_on) {
+        const uint64_t k = std::max<uint64_t>(e->n_start, 1);
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&d->d_start_idx), k * sizeof(uint32_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&d->d_start_val), k * sizeof(double)));
+        if (e->n_start > 0) {
+            MPX_CUDA(cudaMemcpyAsync(d->d_start_idx, e->d_start_idx, e->n_start * sizeof(uint32_t),
+                                     cudaMemcpyDeviceToDevice, d->stream));
+            MPX_CUDA(cudaMemcpyAsync(d->d_start_val, e->d_start_val, e->n_start * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, d->stream));
+        }
+        d->n_start = e->n_start;
+        d->start_on = true;
+    }
+    const FrozenGraph &g = e->fg;
+    if (g.L > 0) {
+        FrozenGraph &h = d->fg;
+        const uint64_t L = g.L;
+        std::vector<uint64_t> begin(L);
+        MPX_CUDA(cudaMemcpyAsync(begin.data(), g.p_begin, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+        uint64_t total = 0;
+        for (uint64_t st = 0; st < L; ++st) total = std::max(total, begin[st] + g.count[st]);
+        const uint64_t n_warps = static_cast<uint64_t>(d->grid) * kWarps;
+        const uint64_t nw = std::max<uint64_t>((g.n_final + 31) / 32, 4);
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.src), std::max<uint64_t>(total, 1) * sizeof(uint32_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.tgt), std::max<uint64_t>(total, 1) * sizeof(uint32_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.code), std::max<uint64_t>(total, 1) * sizeof(int8_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.p_begin), L * sizeof(uint64_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.p_count), L * sizeof(unsigned long long)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.w_anti), L * n_warps * sizeof(uint32_t)));
+        MPX_CUDA(dev_alloc(d, reinterpret_cast<void **>(&h.done), nw * sizeof(uint32_t)));
+        if (total > 0) {
+            MPX_CUDA(cudaMemcpyAsync(h.src, g.src, total * sizeof(uint32_t), cudaMemcpyDeviceToDevice, d->stream));
+            MPX_CUDA(cudaMemcpyAsync(h.tgt, g.tgt, total * sizeof(uint32_t), cudaMemcpyDeviceToDevice, d->stream));
+            MPX_CUDA(cudaMemcpyAsync(h.code, g.code, total * sizeof(int8_t), cudaMemcpyDeviceToDevice, d->stream));
+        }
+        MPX_CUDA(cudaMemcpyAsync(h.p_begin, g.p_begin, L * sizeof(uint64_t), cudaMemcpyDeviceToDevice, d->stream));
+        MPX_CUDA(cudaMemcpyAsync(h.p_count, g.p_count, L * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                 d->stream));
+        MPX_CUDA(cudaMemcpyAsync(h.w_anti, g.w_anti, L * n_warps * sizeof(uint32_t), cudaMemcpyDeviceToDevice, d->stream));
+        MPX_CUDA(cudaMemsetAsync(h.done, 0, nw * sizeof(uint32_t), d->stream));
+        h.L = L;
+        h.n_final = g.n_final;
+        h.n0 = g.n0;
+        h.anti = g.anti;
+        h.count = g.count;
+    }
+    MPX_CUDA(cudaStreamSynchronize(d->stream));
+    return MPX_OK;
+}
+
+}  // namespace
+
+mpx_status mpx_clone(mpx_engine *e, const mpx_circuit *c, mpx_engine **out, mpx_circuit **c_out) {
+    if (e == nullptr || out == nullptr || (c != nullptr && c_out == nullptr)) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    mpx_engine *eng = e;
+    *out = nullptr;
+    if (c_out != nullptr) *c_out = nullptr;
+    if (c != nullptr && c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
+    MPX_CUDA(cudaSetDevice(e->device));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    const int W = e->W;
+    std::vector<uint64_t> ik(std::max<uint64_t>(e->n_init, 1) * W);
+    std::vector<double> ic(std::max<uint64_t>(e->n_init, 1));
+    if (e->n_init > 0) {
+        MPX_CUDA(cudaMemcpy(ik.data(), e->d_init_keys, e->n_init * W * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        MPX_CUDA(cudaMemcpy(ic.data(), e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    mpx_engine *d = nullptr;
+    mpx_status s = create_engine(&e->cfg, e->n_init > 0 ? ik.data() : nullptr, e->n_init > 0 ? ic.data() : nullptr,
+                                 e->n_init, e->core, e->mask.w, &d, !e->keep_blocks);
+    if (s != MPX_OK) return fail(eng, s, mpx_last_error(nullptr));
+    s = clone_into(e, d);
+    if (s == MPX_OK && c != nullptr) {
+        s = mpx_circuit_upload(d, c->words.data(), c->angles.data(), c->n, c_out);
+        if (s == MPX_OK && e->fg.L > 0 && e->fg.circuit_id == c->id) d->fg.circuit_id = (*c_out)->id;
+    }
+    if (s != MPX_OK) {
+        const std::string msg = d->err;
+        if (c_out != nullptr && *c_out != nullptr) {
+            mpx_circuit_destroy(*c_out);
+            *c_out = nullptr;
+        }
+        mpx_destroy(d);
+        return fail(eng, s, "clone failed: " + msg);
+    }
+    *out = d;
+    return MPX_OK;
+}
+
+mpx_status mpx_current_device(int32_t *device) {
+    if (device == nullptr) return fail(nullptr, MPX_ERR_INVALID, "NULL argument");
+    int d = 0;
+    const cudaError_t ce = cudaGetDevice(&d);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, MPX_ERR_NO_DEVICE, std::string("no current CUDA device: ") + cudaGetErrorString(ce));
+    }
+    *device = d;
+    return MPX_OK;
+}
+
 // Internal (not exported): the batch runner's engines, created as sharing the GPU (see create_engine).
 mpx_status mpx_internal_create_shared(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef,
                                       uint64_t n_obs, double core, const uint64_t *state_mask, mpx_engine **out) {
@@ -2007,6 +2399,7 @@ void mpx_destroy(mpx_engine *e) {
     dev_free(e, e->d_init_coef);
     dev_free(e, e->d_basis);
     dev_free(e, e->d_stats);
+    clear_start(e);
     if (e->stream != nullptr) {
         cudaStreamSynchronize(e->stream); // the pool frees above are stream-ordered
         cudaStreamDestroy(e->stream);

@@ -337,10 +337,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
 // each sweep warp's terms are the ones it counted in the forward pass. With LOG every anticommuting
 // term's pre-gate value goes to the undo log from its chunk-owning warp's offset (pair members' entries
 // are never read).
+// With a pared graph (last != nullptr) a term whose value can no longer reach <0|O|0> after this step
+// (last[term] < step) keeps its coefficient unscaled.
 template <int W, bool LOG>
 __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
     k_frozen_scan(Store st, const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step, uint64_t n0,
-                  uint32_t *__restrict__ done, Tape tp) {
+                  uint32_t *__restrict__ done, Tape tp, const int32_t *__restrict__ last) {
     __shared__ uint32_t s_anti[kWarps][kBatch * 32];
     __shared__ uint32_t s_done[kWarps][kBatch * 32];
     __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
@@ -471,7 +473,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                     tp.u_idx[rr] = static_cast<uint32_t>(term[r]);
                     tp.u_val[rr] = vv[r];
                 }
-                if (!skip[r]) st.coef[term[r]] = vv[r] * C;
+                if (!skip[r] && (last == nullptr || last[term[r]] >= static_cast<int32_t>(step)))
+                    st.coef[term[r]] = vv[r] * C;
             }
         }
         __syncthreads(); // the lists of this batch are consumed

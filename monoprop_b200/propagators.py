@@ -98,12 +98,53 @@ class MonomialPropagator:
     def gradient(self, parameters=None):
         return self.expectation_value_and_gradient(parameters)[1]
 
-    def expectation_value_functional(self):
-        """A callable ``parameters -> <O>`` over the stored graph (or the current operator)."""
-        return lambda parameters=None: self.expectation_value(parameters)
+    def expectation_value_functional(self, pare_threshold: float | None = None):
+        """A reusable callable ``parameters -> <O>`` over the stored graph; with ``pare_threshold`` the graph
+        is pared of what cannot reach the reference state (``monomial_propagator.py:380-401``). It goes
+        stale (RuntimeError when called) after build_graph, contract_partially or update_initial_operator."""
+        fn = self._simulator.expectation_value_functional(pare_threshold)
+        return lambda parameters=None: fn(self._bind(parameters))
 
-    def expectation_value_and_gradient_functional(self):
-        return lambda parameters=None: self.expectation_value_and_gradient(parameters)
+    def expectation_value_and_gradient_functional(self, pare_threshold: float | None = None):
+        """Like :meth:`expectation_value_functional`, returning ``(<O>, gradient)``
+        (``monomial_propagator.py:403-428``)."""
+        fn = self._simulator.expectation_value_and_gradient_functional(pare_threshold)
+
+        def _call(parameters=None):
+            value, grad = fn(self._bind(parameters))
+            return value, np.asarray(grad, dtype=np.float64)
+
+        return _call
+
+    @property
+    def parameter_mapping(self) -> list[int]:
+        """Parameter index of every graph layer (``monomial_propagator.py:303-335``); assignable, per layer
+        or per gate, to re-wire the stored graph's parameters."""
+        return list(self._simulator.parameter_mapping)
+
+    @parameter_mapping.setter
+    def parameter_mapping(self, mapping) -> None:
+        resolved = [int(i) for i in mapping]
+        self._simulator.parameter_mapping = resolved
+        self._n_params = max(self._simulator.parameter_mapping, default=-1) + 1
+
+    def n_gates(self) -> int:
+        return self._simulator.n_gates()
+
+    def graph_size(self) -> tuple[int, int]:
+        """(cos-only indices, pairs) of the stored graph (``monomial_propagator.py:560-568``)."""
+        return tuple(self._simulator.graph_size())
+
+    def operator_memory_breakdown(self) -> dict:
+        return dict(self._simulator.operator_memory_breakdown())
+
+    def __deepcopy__(self, memo):
+        import copy
+
+        new = self.__class__.__new__(self.__class__)
+        for k, v in self.__dict__.items():
+            new.__dict__[k] = v.__deepcopy__(memo) if k == "_simulator" else copy.deepcopy(v, memo)
+        return new
 
     expval_functional = expectation_value_functional
     expval_and_grad_functional = expectation_value_and_gradient_functional
@@ -190,6 +231,10 @@ class PauliPropagator(MonomialPropagator):
         terms = {Pauli.from_slots(slots): complex(c) for slots, c in raw.items()}
         return PauliOperator(terms, self.num_qubits)
 
+    def update_initial_operator(self, new_operator: PauliOperator) -> None:
+        """Re-weight the initial operator: its terms must already be stored (``pauli_propagator.py:215-237``)."""
+        self._simulator.update_initial_operator(new_operator.get_local_operator().terms)
+
 
 class MajoranaPropagator(MonomialPropagator):
     """Fermionic propagator over Majorana monomials (``majorana_propagator.py:44-93``)."""
@@ -212,3 +257,15 @@ class MajoranaPropagator(MonomialPropagator):
     def evolved_operator(self, parameters=None, *, atol: float = 1e-12) -> MajoranaOperator:
         raw = self._simulator.evolved_operator(self._bind(parameters), atol)
         return MajoranaOperator(raw, self._system_size)
+
+    def update_initial_operator(self, new_operator) -> None:
+        """Re-weight the initial operator: its terms must already be stored (``majorana_propagator.py:125-142``)."""
+        self._simulator.update_initial_operator(new_operator.get_majorana_operator().terms)
+
+    @property
+    def cutoff_type(self) -> str:
+        return self._simulator.cutoff_type
+
+    @cutoff_type.setter
+    def cutoff_type(self, value: str) -> None:
+        self._simulator.cutoff_type = value

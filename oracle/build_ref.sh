@@ -3,11 +3,13 @@
 # headers/stubs in oracle/ref_shim and oracle/ref_stubs.cpp and the C-ABI driver oracle/ref_driver.cpp,
 # into oracle/_ref/. The reference tree is only read; nothing is copied into this repository.
 #
-# Two builds of the same sources, differing only in the instruction set:
-#   libmpref.so     -march=x86-64-v3 (AVX2/FMA/BMI2): runs on any host CPU of the GPU machines;
-#   libmpref_v4.so  -march=x86-64-v4 (adds AVX-512F/BW/CD/DQ/VL): what the reference's own default build
-#                   (-march=native) selects on an AVX-512 host. The timing arm uses it where the host CPU
-#                   has those extensions and it is the faster of the two.
+# Three builds of the same sources, differing only in the instruction set:
+#   libmpref.so      -march=x86-64-v3 (AVX2/FMA/BMI2): runs on any host CPU of the GPU machines; the oracle
+#                    the tests use;
+#   libmpref_v4.so   -march=x86-64-v4 (adds AVX-512F/BW/CD/DQ/VL);
+#   libmpref_spr.so  -march=sapphirerapids: what the reference's own default build (-march=native,
+#                    cmake/compiler_flags/CXXFlags.cmake) selects on the GPU machines' Sapphire Rapids hosts.
+# The timing arm runs the build matching the host CPU's extensions (the reference's stock flags there).
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: $MONOPROP_REFERENCE, else /root/reference)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -44,3 +46,4 @@ build_variant() { # $1 = -march value, $2 = object dir, $3 = library name
 }
 build_variant x86-64-v3 obj libmpref.so
 build_variant x86-64-v4 obj_v4 libmpref_v4.so
+build_variant sapphirerapids obj_spr libmpref_spr.so

@@ -138,6 +138,32 @@ def full_depth() -> None:
         print("full", name, wl.n_layers, r.keys.shape[0], r.expectation, f"{r.seconds:.1f} s", flush=True)
 
 
+def surface(reference_root: str) -> None:
+    """The names the reference's nanobind module binds per propagator class and module-wide
+    (``src/monoprop/bindings/binder.h``, ``bindings.cpp.in``), and the ``_simulator`` attributes its Python
+    front-end uses (``src/monoprop/*.py``): reference_surface.json, read by tests/test_core_surface.py."""
+    import json
+    import re
+
+    bind = os.path.join(reference_root, "src", "monoprop", "bindings")
+    with open(os.path.join(bind, "binder.h")) as f:
+        binder = f.read()
+    with open(os.path.join(bind, "bindings.cpp.in")) as f:
+        module = f.read()
+    calls = set()
+    src = os.path.join(reference_root, "src", "monoprop")
+    for name in sorted(os.listdir(src)):
+        if name.endswith(".py"):
+            with open(os.path.join(src, name)) as f:
+                calls.update(re.findall(r"_simulator\.(\w+)", f.read()))
+    out = {"class_members": sorted(set(re.findall(r"cls\.def\w*\(\s*\"(\w+)\"", binder))),
+           "module_attributes": sorted(set(re.findall(r"m\.(?:attr|def)\(\s*\"(\w+)\"", module))),
+           "frontend_simulator_calls": sorted(calls)}
+    with open(os.path.join(HERE, "reference_surface.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("surface", {k: len(v) for k, v in out.items()})
+
+
 def main(reference_root: str | None = None) -> None:
     reference_root = reference_root or os.environ.get("MONOPROP_REFERENCE")
     if not reference_root:
@@ -147,6 +173,9 @@ def main(reference_root: str | None = None) -> None:
         raise SystemExit("reference oracle could not be built")
     if "--full-depth" in sys.argv:
         full_depth()
+        return
+    if "--surface" in sys.argv:
+        surface(reference_root)
         return
     for name, make, L, k in LEN_K:
         wl = make()
