@@ -137,6 +137,20 @@ def _cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
+_REF_BUILD = None
+
+
+def ref_build() -> str:
+    """The reference build this host's CPU runs as the reference's stock -march=native build would
+    (oracle.native_ref_build), chosen once per process."""
+    global _REF_BUILD
+    if _REF_BUILD is None:
+        import oracle
+
+        _REF_BUILD = oracle.native_ref_build()
+    return _REF_BUILD
+
+
 def time_reference(wl, steps: int, warmup: int, partitions: int) -> dict:
     """The unmodified reference engine on the host cores: per step, one full propagate of ``wl``.
 
@@ -146,9 +160,10 @@ def time_reference(wl, steps: int, warmup: int, partitions: int) -> dict:
 
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libmpref.so is missing (build it with oracle/build_ref.sh)")
+    build = ref_build()
 
     def run(p, n_layers=None):
-        eng = oracle.RefEngine(wl, partitions=p)
+        eng = oracle.RefEngine(wl, partitions=p, build=build)
         t = eng.propagate(n_layers=n_layers)
         eng.close()
         return t
@@ -160,7 +175,25 @@ def time_reference(wl, steps: int, warmup: int, partitions: int) -> dict:
     if partitions > 1 and run(partitions) < 1.0 and run(1) < run(partitions):
         chosen = 1
     secs = [run(chosen) for _ in range(steps)]
-    return {"seconds": secs, "partitions": chosen}
+    return {"seconds": secs, "partitions": chosen, "build": build}
+
+
+def time_reference_gradient(wl, partitions: int, evals: int = 1) -> dict:
+    """The reference's <O> + full gradient: build_graph once at the workload's parameters
+    (MonomialPropagator.inl:620-690), then ``evals`` calls of expectation_value_and_gradient
+    (MPFunctions.cpp:207-246) on all host threads."""
+    import oracle
+
+    build = ref_build()
+    eng = oracle.RefEngine(wl, partitions=partitions, build=build)
+    try:
+        t_build = eng.propagate(build_graph=True)
+        secs = [eng.expectation_and_gradient(wl.params)[2] for _ in range(evals)]
+    finally:
+        eng.close()
+    return {"value": len(secs) / sum(secs), "unit": "gradients/s", "seconds_per_eval": sum(secs) / len(secs),
+            "build_graph_seconds": t_build, "cores": partitions, "kind": "reference", "build": build,
+            "sample": f"build_graph once, then {evals} expectation_value_and_gradient call(s), partitions={partitions}"}
 
 
 def main() -> None:
@@ -178,6 +211,8 @@ def main() -> None:
                          "Pauli weight <= 10, then the last --case-gates gates of the 10x10 circuit")
     ap.add_argument("--case-gates", type=int, default=4)
     ap.add_argument("--no-gradient", action="store_true", help="skip the <O> + full-gradient measurement")
+    ap.add_argument("--no-sub-results", action="store_true",
+                    help="skip the compact measurements of the 20-qubit line and 6x6 Hubbard circuits")
     ap.add_argument("--segment-layers", type=int, default=4,
                     help="gradient checkpoint interval in circuit layers (the circuit repeats one layer of gates)")
     args = ap.parse_args()
@@ -215,8 +250,12 @@ def main() -> None:
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded circuit)", "config": config, "impl": "reference",
                 "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "reference",
-                                 "sample": f"full {wl.name} propagate per step, partitions={t['partitions']}"},
+                                 "build": t["build"],
+                                 "sample": f"full {wl.name} propagate per step, partitions={t['partitions']}, "
+                                           f"reference built for the host CPU ({t['build']})"},
                 "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not args.no_gradient:
+            line["gradient"] = time_reference_gradient(wl, cores)
         print(json.dumps(line), flush=True)
         return
 
@@ -278,6 +317,7 @@ def main() -> None:
     if dist is not None:
         dist.barrier()
     launches = eng.launch_count() - launches0
+    graph_replays = eng.graph_replay_count()
     # Per-kernel device times from the same number of steps again, each kernel launch bracketed by CUDA
     # events on the engine stream (the events themselves cost time, so these steps are not the value).
     sweep_ms, resolve_ms = [], []
@@ -316,6 +356,13 @@ def main() -> None:
                      "ms_per_eval": g_per, "forward_ms": ms_per_step, "cost_vs_forward": g_per / ms_per_step,
                      "segment_gates": seg, "n_angles": int(wl.n_layers), "expectation": ev_g,
                      "grad_abs_max": float(np.max(np.abs(grad)))}
+
+    # The other two circuits of the task (the 20-qubit line and the 6x6 Hubbard circuit), measured the same
+    # way on this GPU (one rank only: no collective takes part).
+    sub_results = []
+    if world == 1 and not args.no_sub_results:
+        for name in ("line20", "hubbard6x6"):
+            sub_results.append(measure_compact(WL.BY_NAME[name](), max(args.steps, 5), args.warmup, local, flush))
 
     # End to end through the C ABI with host buffers (create + propagate + expectation + destroy).
     e2e_ms = []
@@ -374,8 +421,19 @@ def main() -> None:
             t = time_reference(wl, 1, 0, cores)
             secs = t["seconds"]
             cpu = {"value": updates / secs[0], "unit": "updates/s", "cores": cores, "kind": "reference",
+                   "build": t["build"],
                    "sample": f"one full {wl.name} propagate (all {wl.n_layers} gates), "
-                             f"partitions={t['partitions']}", "seconds": secs[0]}
+                             f"partitions={t['partitions']}, reference built for the host CPU ({t['build']})",
+                   "seconds": secs[0]}
+            if grad_line is not None:
+                grad_line["cpu_reference"] = time_reference_gradient(wl, cores)
+            if not args.no_sub_results:
+                for sub in sub_results:
+                    st = time_reference(WL.BY_NAME[sub["workload"]](), 3, 1, cores)
+                    sub["cpu_baseline"] = {"value": _updates(WL.BY_NAME[sub["workload"]]()) * 3 / sum(st["seconds"]),
+                                           "unit": "updates/s", "cores": cores, "kind": "reference",
+                                           "build": st["build"], "partitions": st["partitions"],
+                                           "sample": "3 full propagates"}
         else:
             cpu = {"value": None, "unit": "updates/s", "cores": 0, "kind": "reference",
                    "sample": "oracle/_ref/libmpref.so not built"}
@@ -387,12 +445,62 @@ def main() -> None:
             "expectation": ev_dev, "expectation_e2e": ev2,
             "e2e": {"value": e2e, "unit": "updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8,
                     "ms_per_step": e2e_total / args.steps},
-            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gradient": grad_line}
+            "gpu_launches": launches, "graph_replays": graph_replays, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "gradient": grad_line, "sub_results": sub_results}
     print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def measure_compact(wl, steps: int, warmup: int, device: int, flush) -> dict:
+    """Device rate of one resident circuit (store reset untimed, L2 flushed, CUDA events on the engine's
+    stream) and its end-to-end rate through the C ABI from host buffers, as for the main workload."""
+    import torch
+
+    from monoprop_b200 import _native
+
+    dev = torch.device("cuda", device)
+    gw, ang = wl.gen_words(), wl.angles()
+    eng = _native.engine_for(wl, device=device)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
+    circ = eng.upload(gw, ang)
+    ms = []
+    for i in range(warmup + steps):
+        eng.reset()
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.propagate_circuit(circ)
+        b.record(stream)
+        b.synchronize()
+        if i >= warmup:
+            ms.append(a.elapsed_time(b))
+    updates = eng.gate_stats().term_gate_updates
+    ev = eng.expectation()
+    circ.close()
+    eng.close()
+    e2e_ms = []
+    for i in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2 = _native.engine_for(wl, device=device)
+        e2.propagate(gw, ang)
+        e2.expectation()
+        e2.close()
+        if i >= warmup:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    keys, coefs, _ = wl.encoded_observable()
+    return {"workload": wl.name, "config": f"{wl.num_modes} modes, {wl.n_layers} gates, {wl.basis}, cutoff {wl.cutoff}, "
+                                          f"lower_atol {wl.lower_atol}",
+            "metric": "term-gate updates/s", "value": updates * len(ms) / (sum(ms) * 1e-3), "unit": "updates/s",
+            "ms_per_step": sum(ms) / len(ms), "steps": len(ms), "expectation": ev,
+            "e2e": {"value": updates * len(e2e_ms) / (sum(e2e_ms) * 1e-3), "unit": "updates/s",
+                    "ms_per_step": sum(e2e_ms) / len(e2e_ms),
+                    "h2d_bytes_per_step": int(gw.nbytes + ang.nbytes + keys.nbytes + coefs.nbytes),
+                    "d2h_bytes_per_step": 8}}
 
 
 def batch_bench(args) -> None:

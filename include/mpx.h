@@ -145,6 +145,12 @@ MPX_API mpx_status mpx_stream(mpx_engine *e, void **stream);
 /* Number of engine kernel launches issued since the engine was created. */
 MPX_API mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out);
 
+/* Number of propagations of a resident circuit (mpx_circuit_upload) whose streaming gate range ran as one
+ * replayed CUDA graph. A range is captured after a propagation that did not grow the store (from the gate
+ * where the shared-memory path handed over) and replayed while the store, its scratch and the truncation
+ * settings are unchanged. No reference counterpart (the reference is host-only). */
+MPX_API mpx_status mpx_graph_replay_count(mpx_engine *e, uint64_t *out);
+
 /* Gradient of <0|O|0> with respect to every gate angle (reverse mode over the frozen truncation structure
  * of the forward pass). Replaces the reference's graph build + replayed gradient,
  * MonomialPropagator<N>::build_graph (MonomialPropagator.inl:620-690) followed by

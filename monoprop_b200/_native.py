@@ -27,7 +27,8 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_graph_gradient", "mpx_set_pair_log", "mpx_set_profiling", "mpx_kernel_times",
             "mpx_trim_device_memory", "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run", "mpx_update_initial_operator", "mpx_memory",
-            "mpx_graph_info", "mpx_clone", "mpx_current_device", "mpx_graph_pare", "mpx_set_cutoff_type")
+            "mpx_graph_info", "mpx_clone", "mpx_current_device", "mpx_graph_pare", "mpx_set_cutoff_type",
+            "mpx_graph_replay_count")
 
 
 class MpxError(RuntimeError):
@@ -113,6 +114,7 @@ def load() -> C.CDLL:
             "mpx_current_device": (st, [C.POINTER(C.c_int32)]),
             "mpx_graph_pare": (st, [vp, vp, C.c_double]),
             "mpx_set_cutoff_type": (st, [vp, C.c_int32]),
+            "mpx_graph_replay_count": (st, [vp, C.POINTER(u64)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -279,6 +281,12 @@ class Engine:
     def launch_count(self) -> int:
         out = C.c_uint64(0)
         self._check(self.lib.mpx_launch_count(self.h, C.byref(out)))
+        return int(out.value)
+
+    def graph_replay_count(self) -> int:
+        """Propagations of a resident circuit that ran their streaming gates as one replayed CUDA graph."""
+        out = C.c_uint64(0)
+        self._check(self.lib.mpx_graph_replay_count(self.h, C.byref(out)))
         return int(out.value)
 
     def adjoint_forward(self, circuit: Circuit, segment_gates: int = 0) -> float:

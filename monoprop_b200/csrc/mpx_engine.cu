@@ -113,6 +113,7 @@ struct mpx_engine {
     double *d_out = nullptr;
     double *h_out = nullptr; // pinned
     uint64_t launches = 0;
+    uint64_t graph_replays = 0; // gate ranges run as one captured CUDA graph
     // Per-kernel event timing (mpx_set_profiling): start/stop events around every sweep and resolve
     // launch of the last propagate call, summed on the host afterwards.
     int profile = 0;
@@ -858,7 +859,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
     bool pending = false;
     uint64_t pending_slot = 0;
     // Small store: run gates in one shared-memory block until the store outgrows it (or the range ends).
-    bool used_small = false;
+
     if (e->small_path && e->W <= 4 && !e->profile && !cd.any_cos_zero && !e->tr.has_len_k && e->tr.basis_rows == nullptr &&
         e->fwd_tape.w_anti == nullptr &&
         hi - lo >= 8) {
@@ -890,23 +891,27 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
             c.err = e->h_cnt->err; // a table inconsistency of the shared-memory path is reported below
             MPX_CUDA(cudaMemcpyAsync(e->d_cnt, &c, sizeof(Counters), cudaMemcpyHostToDevice, e->stream));
             step = resume;
-            used_small = true;
+
         }
     }
     const uint64_t gen0 = e->store_gen;
     // A gradient's forward pass is not captured: its tape buffers are allocated per call, so a captured
     // range would rarely match the next call's pointers and each miss would pay a new capture.
-    const bool graphable = e->use_graphs && !e->profile && cd.persistent && !used_small && e->fwd_tape.w_anti == nullptr;
+    // The streaming part of the range, [glo, hi): after the shared-memory path, from the gate it handed
+    // over at (the same gate on every call with the same circuit, angles and initial operator).
+    const uint64_t glo = step;
+    const bool graphable = e->use_graphs && !e->profile && cd.persistent && e->fwd_tape.w_anti == nullptr && glo < hi;
     bool replayed = false;
     if (graphable) {
         for (const auto &g : e->graphs) {
-            if (g.circuit_id != cd.id || g.lo != lo || g.hi != hi || g.gen != gen0 || g.w_anti != e->fwd_tape.w_anti ||
+            if (g.circuit_id != cd.id || g.lo != glo || g.hi != hi || g.gen != gen0 || g.w_anti != e->fwd_tape.w_anti ||
                 g.r_src != e->fwd_tape.r_src || g.r_cap != e->fwd_tape.r_cap)
                 continue;
             // One launch for the whole range; a gate that would overflow stalls the rest (no-ops), and the
             // host resumes from it below exactly as after a chunk.
             MPX_CUDA(cudaGraphLaunch(g.exec, e->stream));
-            e->launches += 2 * (hi - lo);
+            e->launches += 2 * (hi - glo);
+            ++e->graph_replays;
             MPX_CUDA(cudaMemcpyAsync(&e->h_snap[0], e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
             MPX_CUDA(cudaEventRecord(e->ev[0], e->stream));
             step = hi;
@@ -973,7 +978,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
         cudaGraphExec_t exec = nullptr;
         bool ok = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            for (uint64_t st = lo; st < hi; ++st) gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
+            for (uint64_t st = glo; st < hi; ++st) gate(e, cd.d_desc, static_cast<uint32_t>(L - 1 - st), static_cast<uint32_t>(st));
             ok = cudaStreamEndCapture(e->stream, &graph) == cudaSuccess && graph != nullptr;
         }
         ok = ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
@@ -983,7 +988,7 @@ mpx_status run_range(mpx_engine *eng, const CircuitDev &cd, uint64_t lo, uint64_
                 cudaGraphExecDestroy(e->graphs.front().exec);
                 e->graphs.erase(e->graphs.begin());
             }
-            e->graphs.push_back({cd.id, lo, hi, gen0, e->fwd_tape.w_anti, e->fwd_tape.r_src, e->fwd_tape.r_cap, exec});
+            e->graphs.push_back({cd.id, glo, hi, gen0, e->fwd_tape.w_anti, e->fwd_tape.r_src, e->fwd_tape.r_cap, exec});
         }
         else {
             e->use_graphs = false; // capture unavailable here: keep issuing kernels directly
@@ -1976,6 +1981,12 @@ mpx_status mpx_stream(mpx_engine *e, void **stream) {
 mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out) {
     if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     *out = e->launches;
+    return MPX_OK;
+}
+
+mpx_status mpx_graph_replay_count(mpx_engine *e, uint64_t *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    *out = e->graph_replays;
     return MPX_OK;
 }
 

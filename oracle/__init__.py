@@ -102,10 +102,53 @@ def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 
 
-def _load_ref() -> C.CDLL:
+#: builds of the reference by instruction set (oracle/build_ref.sh), most specific first, with the host CPU
+#: flags each needs
+REF_BUILDS = {
+    "spr": (os.path.join(HERE, "_ref", "libmpref_spr.so"),
+            ("avx512f", "avx512bw", "avx512vl", "avx512dq", "avx512cd", "avx512_fp16", "avx512_bf16", "amx_tile",
+             "avx512_vpopcntdq", "avx512_bitalg", "avx512vbmi", "avx512_vbmi2", "avx512_vnni", "gfni", "vaes")),
+    "v4": (os.path.join(HERE, "_ref", "libmpref_v4.so"), ("avx512f", "avx512bw", "avx512vl", "avx512dq", "avx512cd")),
+    "v3": (REF_LIB, ("avx2", "fma", "bmi2")),
+}
+
+
+def _host_flags() -> set[str]:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def native_ref_build() -> str:
+    """The reference build matching this host's CPU, as the reference's own default -march=native build
+    would (``cmake/compiler_flags/CXXFlags.cmake``): the most specific one whose instruction-set extensions
+    the host has and whose library was built, checked by a short run in a child process (an illegal
+    instruction there cannot take this process down)."""
+    import subprocess
+    import sys
+
+    flags = _host_flags()
+    for name, (path, need) in REF_BUILDS.items():
+        if name == "v3" or not os.path.exists(path) or not all(f in flags for f in need):
+            continue
+        probe = ("import sys; sys.path.insert(0, %r); import oracle; from monoprop_b200 import workloads as W; "
+                 "oracle.RefEngine(W.line20(), build=%r).propagate(n_layers=40)") % (os.path.dirname(HERE), name)
+        if subprocess.run([sys.executable, "-c", probe], capture_output=True, timeout=120).returncode == 0:
+            return name
+    return "v3"
+
+
+def _load_ref(build: str = "v3") -> C.CDLL:
     global _ref
     if _ref is None:
-        lib = C.CDLL(REF_LIB)
+        _ref = {}
+    if build not in _ref:
+        lib = C.CDLL(REF_BUILDS[build][0])
         lib.mpref_create.restype = C.c_void_p
         lib.mpref_create.argtypes = [C.POINTER(_RefCfg), C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p,
@@ -129,8 +172,8 @@ def _load_ref() -> C.CDLL:
         lib.mpref_export.restype = C.c_int64
         lib.mpref_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t]
         lib.mpref_destroy.argtypes = [C.c_void_p]
-        _ref = lib
-    return _ref
+        _ref[build] = lib
+    return _ref[build]
 
 
 def _basis_code(basis: str) -> int:
@@ -196,8 +239,8 @@ def _flat_slots(monos) -> tuple[np.ndarray, np.ndarray]:
 class RefEngine:
     """The unmodified reference ``MonomialPropagator<N>`` through the C-ABI driver."""
 
-    def __init__(self, wl, partitions: int = 1):
-        self.lib = _load_ref()
+    def __init__(self, wl, partitions: int = 1, build: str = "v3"):
+        self.lib = _load_ref(build)
         self.wl = wl
         obs = sorted(wl.observable.items())
         off, flat = _flat_slots([k for k, _ in obs])

@@ -89,6 +89,33 @@ def test_reset_and_resident_circuit_with_new_angles():
     assert abs(ev - ref.expectation) <= 1e-10 * max(1.0, abs(ref.expectation))
 
 
+def test_resident_circuit_replays_a_captured_cuda_graph():
+    """The 100-qubit circuit's first 1200 gates, resident: the first propagation grows the store, the
+    second (no growth) captures the streaming gate range after the shared-memory hand-off, the third
+    replays it as one CUDA graph. All three give the reference's store (keys bit-exact, coefficients
+    bit-identical per key)."""
+    wl = W.ising100()
+    L = 1200
+    g = golden.load("ising100_L1200")
+    eng = _native.engine_for(wl)
+    circ = eng.upload(wl.gen_words()[:L], wl.angles()[:L])
+    runs = []
+    for _ in range(3):
+        eng.reset()
+        eng.propagate_circuit(circ)
+        keys, coefs = eng.export()
+        runs.append((keys, coefs, eng.expectation()))
+    replays = eng.graph_replay_count()
+    circ.close()
+    eng.close()
+    assert replays == 1
+    for keys, coefs, ev in runs:
+        golden.check_against(g, keys, coefs, ev)
+    (k0, c0, _), (k2, c2, _) = runs[0], runs[2]
+    i0, i2 = canonical_order(k0), canonical_order(k2)
+    assert np.array_equal(k0[i0], k2[i2]) and np.array_equal(c0[i0], c2[i2])
+
+
 def test_growth_from_tiny_capacity_matches_presized():
     wl = W.ising50(3)
     k1, c1, e1 = run_engine(wl, capacity_hint=1)
