@@ -57,6 +57,15 @@ typedef struct {
     int32_t blocks_per_sm;  /* tuning: per-gate kernel grid, blocks per SM (1..4); 0 = 4 */
     int32_t table_shift;    /* tuning: hash table slots = next_pow2(capacity << table_shift) (1..3): load
                                factor <= 1/2, 1/4, 1/8; 0 = 1 */
+    /* Schrodinger picture (kwarg schrodinger_cutoff=, MonomialPropagator.inl:146-179): when
+     * has_schrodinger, the store starts as every fully paired monomial of at most
+     * ceil(min(schrodinger_cutoff, 2 * logical modes) / 2) mode pairs over the logical modes, each holding its
+     * reference-state score (generate_paired_op, MajoranaAlgebra.h:127-160); the observable is kept apart,
+     * gates run first to last at the negated angle, an appended partner starts from its score
+     * (FusedApply.h:39-83), and <O> = core + observable . state (MPFunctions.cpp:196-205). */
+    int32_t has_schrodinger;
+    int32_t schrodinger_cutoff;
+    int32_t logical_num_modes; /* modes the paired initial state spans (0 = num_modes) */
 } mpx_config;
 
 typedef struct mpx_engine mpx_engine;

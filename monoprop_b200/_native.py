@@ -47,7 +47,8 @@ class Config(C.Structure):
     _fields_ = [("basis", C.c_int32), ("cutoff_type", C.c_int32), ("cutoff", C.c_uint32),
                 ("has_lower_atol", C.c_int32), ("lower_atol", C.c_double), ("has_upper_atol", C.c_int32),
                 ("upper_atol", C.c_double), ("num_modes", C.c_int32), ("device", C.c_int32),
-                ("capacity_hint", C.c_uint64), ("blocks_per_sm", C.c_int32), ("table_shift", C.c_int32)]
+                ("capacity_hint", C.c_uint64), ("blocks_per_sm", C.c_int32), ("table_shift", C.c_int32),
+                ("has_schrodinger", C.c_int32), ("schrodinger_cutoff", C.c_int32), ("logical_num_modes", C.c_int32)]
 
 
 class MemoryInfo(C.Structure):
@@ -180,12 +181,16 @@ class Engine:
     def __init__(self, *, basis: str, cutoff_type: str, cutoff: int, num_modes: int,
                  keys: np.ndarray, coefs: np.ndarray, core: float, state_mask: np.ndarray,
                  lower_atol: float | None = None, upper_atol: float | None = None, device: int = 0,
-                 capacity_hint: int = 0, blocks_per_sm: int = 0, table_shift: int = 0):
+                 capacity_hint: int = 0, blocks_per_sm: int = 0, table_shift: int = 0,
+                 schrodinger_cutoff: int | None = None):
+        """``schrodinger_cutoff`` (slots): the Schrodinger picture -- the store starts as the paired
+        reference-state monomials and ``keys``/``coefs`` is the observable dotted into the evolved state."""
         self.lib = load()
         cfg = Config(1 if basis == "pauli" else 0, 1 if cutoff_type == "support" else 0, int(cutoff),
                      int(lower_atol is not None), float(lower_atol or 0.0), int(upper_atol is not None),
                      float(upper_atol or 0.0), int(num_modes), int(device), int(capacity_hint),
-                     int(blocks_per_sm), int(table_shift))
+                     int(blocks_per_sm), int(table_shift), int(schrodinger_cutoff is not None),
+                     int(schrodinger_cutoff or 0), int(num_modes))
         self.words = (int(num_modes) + 31) // 32
         self.num_modes = int(num_modes)
         k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1, self.words)
@@ -348,6 +353,8 @@ class Engine:
 def engine_for(wl, **kw) -> Engine:
     """Engine holding workload ``wl``'s observable (see :mod:`monoprop_b200.workloads`)."""
     keys, coefs, core = wl.encoded_observable()
+    if wl.extra.get("schrodinger_cutoff") is not None:
+        kw.setdefault("schrodinger_cutoff", int(wl.extra["schrodinger_cutoff"]))
     eng = Engine(basis=wl.basis, cutoff_type=wl.cutoff_type, cutoff=wl.cutoff, num_modes=wl.num_modes,
                  keys=keys, coefs=coefs, core=core, state_mask=wl.state_mask(), lower_atol=wl.lower_atol,
                  upper_atol=wl.upper_atol, **kw)

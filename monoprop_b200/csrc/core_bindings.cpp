@@ -104,8 +104,6 @@ public:
         // same results; it is accepted for drop-in compatibility and otherwise unused.
         (void)partitions;
         if (!comm.is_none()) throw NotSupported("comm: the B200 engine runs on one GPU and takes no communicator");
-        if (schrodinger_cutoff.has_value())
-            throw NotSupported("schrodinger_cutoff: the B200 engine implements the Heisenberg picture");
         if (logical_ == 0 || logical_ > Tier)
             throw PropagatorConfigError("logical_num_modes (" + std::to_string(logical_) + ") must be in the range [1, " +
                                         std::to_string(Tier) + "].");
@@ -138,6 +136,11 @@ public:
         cfg_.num_modes = static_cast<int32_t>(Tier);
         cfg_.device = current_device();
         cfg_.capacity_hint = 0;
+        // Schrodinger picture (MonomialPropagator.inl:146-179): the engine builds the paired initial state
+        // over the logical modes and keeps this operator apart for <O> = core + operator . state
+        cfg_.has_schrodinger = schrodinger_cutoff.has_value() ? 1 : 0;
+        cfg_.schrodinger_cutoff = static_cast<int32_t>(schrodinger_cutoff.value_or(0));
+        cfg_.logical_num_modes = static_cast<int32_t>(logical_);
 
         std::vector<uint64_t> keys;
         std::vector<double> coefs;
@@ -277,8 +280,22 @@ public:
         }
         ++graph_epoch_;
         double ev = 0.0;
-        py::gil_scoped_release nogil;
-        check(mpx_graph_build(e_, circ_, 0, &ev), e_);
+        mpx_status st;
+        {
+            py::gil_scoped_release nogil;
+            st = mpx_graph_build(e_, circ_, 0, &ev);
+        }
+        if (st != MPX_OK) { // no graph is kept after a failed build
+            const std::string msg = mpx_last_error(e_);
+            mpx_circuit_destroy(circ_);
+            circ_ = nullptr;
+            mapping_.clear();
+            gen_.clear();
+            gate_of_layer_.clear();
+            n_params_ = gates_ = 0;
+            if (st == MPX_ERR_INVALID) throw std::invalid_argument(msg);
+            throw std::runtime_error(msg);
+        }
     }
 
     // expectation_value_functional / expectation_value_and_gradient_functional (binder.h:137-146,
@@ -545,7 +562,7 @@ public:
             for (size_t s : idx) key.append(s);
             out[py::tuple(key)] = c;
         }
-        if (std::abs(core_) >= atol) out[py::tuple()] = std::complex<double>(core_, 0.0);
+        if (!cfg_.has_schrodinger && std::abs(core_) >= atol) out[py::tuple()] = std::complex<double>(core_, 0.0);
         return out;
     }
 
@@ -587,6 +604,7 @@ public:
         cfg_.cutoff_type = code;
     }
     std::string basis() const { return cfg_.basis == MPX_BASIS_PAULI ? "pauli" : "majorana"; }
+    bool schrodinger() const { return cfg_.has_schrodinger != 0; }
     size_t num_modes() const { return logical_; }
     double core_term() const { return core_; }
     size_t operator_memory_bytes() { return operator_memory_breakdown().at("total_bytes"); }
@@ -758,7 +776,7 @@ void bind(py::module_ &m) {
         .def_property("basis_change", &P::basis_change, &P::set_basis_change)
         .def_property_readonly("basis", &P::basis)
         .def_property_readonly("num_modes", &P::num_modes)
-        .def_property_readonly("schrodinger", [](P &) { return false; })
+        .def_property_readonly("schrodinger", [](P &p) { return p.schrodinger(); })
         .def_property_readonly_static("storage_num_modes", [](py::object) { return Tier; });
 }
 

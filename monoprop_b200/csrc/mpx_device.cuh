@@ -32,6 +32,10 @@ struct GateDesc {
     uint16_t fold_cols[kMaxFoldCols]; // their physical bit indices, when n_fold <= kMaxFoldCols
 };
 
+struct StateMask {
+    uint64_t w[kMaxWords]; // slot 2m set for every occupied mode m of the reference state
+};
+
 // Engine-wide truncation settings (CutoffContext.h:20-42, AlgebraCommon.h:229-243).
 struct Trunc {
     int32_t cutoff_type; // 0 length, 1 support
@@ -43,6 +47,10 @@ struct Trunc {
     uint32_t len_k;
     // basis_change (Majorana): [2T][W] device rows by slot; the partner's cutoff is judged on its image
     const uint64_t *basis_rows;
+    // Schrodinger picture: an appended partner starts from its reference-state score over `occ`
+    // (FusedApply.h:39-83) instead of 0
+    int32_t schr;
+    StateMask occ;
 };
 
 // Programmatic dependent launch (sm_90+): the per-gate kernels let the next kernel of the stream be
@@ -59,10 +67,6 @@ struct Counters {
     uint32_t stall;        // kNoStall, or the step index at which capacity ran out
     uint32_t err;          // nonzero: a bounded probe loop gave up (table inconsistent); results invalid
     unsigned long long rec_total; // pair records written by a recording forward pass (may exceed capacity)
-};
-
-struct StateMask {
-    uint64_t w[kMaxWords]; // slot 2m set for every occupied mode m of the reference state
 };
 
 // The key store is kept twice: as rows (keys, for the per-term work) and as bit-columns (cols, for the
@@ -231,6 +235,23 @@ __device__ __forceinline__ int rotation_phase(const uint64_t (&m)[W], const uint
         const int real = power == 0 ? 1 : (power == 2 ? -1 : 0);
         return (__popcll(par) & 1) ? -real : real;
     }
+}
+
+// Reference-state score <b|M|b> of a key: 0 unless fully paired; then Pauli (-1)^{|M & occ|}, Majorana
+// (-1)^{|M & occ| + |M|/2} (MPOperator.h:235-254, PauliAlgebra.h:144-147, MajoranaAlgebra.h:56-60).
+template <int W, int BASIS>
+__device__ __forceinline__ double state_score(const uint64_t (&m)[W], const StateMask &occ) {
+    uint64_t unpaired = 0;
+    int na = 0, pop = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        unpaired |= (m[w] & kEven) ^ ((m[w] >> 1) & kEven);
+        na += __popcll(m[w] & occ.w[w]);
+        pop += __popcll(m[w]);
+    }
+    if (unpaired != 0) return 0.0;
+    const int odd = BASIS == 1 ? (na & 1) : ((na + pop / 2) & 1);
+    return odd ? -1.0 : 1.0;
 }
 
 __device__ __forceinline__ uint8_t phase_code(int phase) { return phase > 0 ? 0 : (phase < 0 ? 1 : 2); }

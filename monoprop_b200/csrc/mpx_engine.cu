@@ -143,6 +143,12 @@ struct mpx_engine {
     double *d_start_val = nullptr;
     uint64_t n_start = 0;
     bool start_on = false;
+    // Schrodinger picture: the store holds the evolved state; the observable is kept apart for <O>
+    bool schr = false;
+    uint64_t *d_obs_keys = nullptr;
+    double *d_obs_coef = nullptr;
+    uint32_t *d_obs_idx = nullptr;
+    uint64_t n_obs = 0;
     // Large blocks through the kept-block cache (dev_alloc). The batch runner turns it off for its
     // engines: with several engines growing at once, power-of-two classes and idle kept blocks crowd
     // the device, and a 96-instance gradient batch took 2x longer with them.
@@ -156,6 +162,9 @@ struct mpx_engine {
 namespace {
 
 std::atomic<uint64_t> g_circuit_ids{1};
+
+// Largest initial Schrodinger state the engine builds (paired monomials; 8W + 8 bytes each on the device).
+constexpr uint64_t kMaxPairedTerms = uint64_t(1) << 28;
 
 #define MPX_CUDA(call)                                                                                              \
     do {                                                                                                            \
@@ -807,11 +816,25 @@ void make_desc(const mpx_engine *e, const uint64_t *g, double angle, GateDesc &d
     d.inv_cos = c != 0.0 ? 1.0 / c : 1.0;
 }
 
+// Device descriptors of a circuit, in the order the kernels take them: the gates are applied from the
+// last descriptor to the first. Heisenberg applies the circuit's last gate first (MonomialPropagator.inl:
+// 720-733), so descriptor l is gate l. The Schrodinger picture applies the first gate first at the negated
+// angle (MonomialPropagator.inl:595-620, parameters mapped with phase -1, MPFunctions.cpp:186-193), so
+// descriptor l is gate n-1-l with angle -angle.
+void make_descs(const mpx_engine *e, const uint64_t *gen_words, const double *angles, uint64_t n,
+                std::vector<GateDesc> &h) {
+    h.resize(n);
+    for (uint64_t l = 0; l < n; ++l) {
+        const uint64_t gi = e->schr ? n - 1 - l : l;
+        make_desc(e, gen_words + gi * e->W, e->schr ? -angles[gi] : angles[gi], h[l]);
+    }
+}
+
 mpx_status upload_circuit(mpx_engine *eng, const uint64_t *gen_words, const double *angles, uint64_t n,
                           CircuitDev &cd) {
     mpx_engine *e = eng;
-    std::vector<GateDesc> h(n);
-    for (uint64_t l = 0; l < n; ++l) make_desc(e, gen_words + l * e->W, angles[l], h[l]);
+    std::vector<GateDesc> h;
+    make_descs(e, gen_words, angles, n, h);
     MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&cd.d_desc), std::max<uint64_t>(n, 1) * sizeof(GateDesc)));
     if (n > 0) {
         MPX_CUDA(cudaMemcpyAsync(cd.d_desc, h.data(), n * sizeof(GateDesc), cudaMemcpyHostToDevice, e->stream));
@@ -1617,6 +1640,10 @@ mpx_status validate_cfg(const mpx_config *c) {
                     "Pauli encoding).");
     if (c->has_lower_atol && c->has_upper_atol && c->upper_atol < c->lower_atol)
         return fail(nullptr, MPX_ERR_STATE, "upper_atol must be greater than or equal to lower_atol.");
+    if (c->logical_num_modes < 0 || c->logical_num_modes > c->num_modes)
+        return fail(nullptr, MPX_ERR_INVALID, "logical_num_modes must be in the range [0, num_modes].");
+    if (c->has_schrodinger && c->schrodinger_cutoff < 0)
+        return fail(nullptr, MPX_ERR_INVALID, "schrodinger_cutoff must be non-negative.");
     return MPX_OK;
 }
 
@@ -1634,12 +1661,76 @@ namespace {
 // buffer on it allocates straight from the pool (no kept-block cache) and launches without programmatic
 // dependent launch (a kernel scheduled early would hold SM slots at its dependency wait that another
 // engine's ready kernel could use).
+// The Schrodinger picture's initial state (MonomialPropagator.inl:162-165, generate_paired_op
+// MajoranaAlgebra.h:127-160): every fully paired monomial of at most K = sc/2 + sc%2 mode pairs over the
+// L logical modes, sc = min(schrodinger_cutoff, 2L), by subset size and then in lexicographic order of the
+// modes, each holding its reference-state score <b|M|b> (+-1).
+mpx_status paired_store(const mpx_config *cfg, const uint64_t *state_mask, std::vector<uint64_t> &keys,
+                        std::vector<double> &coefs) {
+    const int W = (cfg->num_modes + 31) / 32;
+    const int L = cfg->logical_num_modes > 0 ? cfg->logical_num_modes : cfg->num_modes;
+    const int sc = std::min(cfg->schrodinger_cutoff, 2 * L);
+    const int K = std::min(sc / 2 + sc % 2, L);
+    double total = 0.0, binom = 1.0; // sum_{k <= K} C(L, k)
+    for (int k = 0; k <= K; ++k) {
+        total += binom;
+        binom = binom * (L - k) / (k + 1);
+    }
+    if (total > static_cast<double>(kMaxPairedTerms))
+        return fail(nullptr, MPX_ERR_CAPACITY, "schrodinger_cutoff=" + std::to_string(cfg->schrodinger_cutoff) +
+                                                   " gives an initial state of " + std::to_string(total) +
+                                                   " paired monomials, above the engine's limit of " +
+                                                   std::to_string(kMaxPairedTerms));
+    keys.reserve(static_cast<size_t>(total) * W);
+    coefs.reserve(static_cast<size_t>(total));
+    std::vector<int> sel(static_cast<size_t>(std::max(K, 1)));
+    for (int k = 0; k <= K; ++k) {
+        for (int i = 0; i < k; ++i) sel[i] = i;
+        for (;;) {
+            uint64_t m[kMaxWords] = {};
+            for (int i = 0; i < k; ++i)
+                for (int slot = 2 * sel[i]; slot <= 2 * sel[i] + 1; ++slot) {
+                    const int bit = 64 * W - 1 - slot;
+                    m[bit / 64] |= 1ULL << (bit % 64);
+                }
+            int na = 0, pop = 0;
+            for (int w = 0; w < W; ++w) {
+                na += __builtin_popcountll(m[w] & (state_mask != nullptr ? state_mask[w] : 0ULL));
+                pop += __builtin_popcountll(m[w]);
+            }
+            const int odd = cfg->basis == MPX_BASIS_PAULI ? (na & 1) : ((na + pop / 2) & 1);
+            keys.insert(keys.end(), m, m + W);
+            coefs.push_back(odd ? -1.0 : 1.0);
+            int i = k - 1;
+            while (i >= 0 && sel[i] == L - k + i) --i;
+            if (i < 0) break;
+            ++sel[i];
+            for (int j = i + 1; j < k; ++j) sel[j] = sel[j - 1] + 1;
+        }
+    }
+    return MPX_OK;
+}
+
 mpx_status create_engine(const mpx_config *cfg, const uint64_t *obs_words, const double *obs_coef, uint64_t n_obs,
                          double core, const uint64_t *state_mask, mpx_engine **out, bool shared) {
     if (out == nullptr) return fail(nullptr, MPX_ERR_INVALID, "out is NULL");
     *out = nullptr;
     mpx_status s = validate_cfg(cfg);
     if (s != MPX_OK) return s;
+    // The initial store: the observable (Heisenberg), or the paired reference-state monomials with the
+    // observable kept apart (Schrodinger).
+    std::vector<uint64_t> paired_keys;
+    std::vector<double> paired_coef;
+    const uint64_t *init_words = obs_words;
+    const double *init_coef = obs_coef;
+    uint64_t n_init_terms = n_obs;
+    if (cfg->has_schrodinger) {
+        s = paired_store(cfg, state_mask, paired_keys, paired_coef);
+        if (s != MPX_OK) return s;
+        init_words = paired_keys.data();
+        init_coef = paired_coef.data();
+        n_init_terms = paired_coef.size();
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -1668,7 +1759,7 @@ mpx_status create_engine(const mpx_config *cfg, const uint64_t *obs_words, const
     e->core = core;
     for (int w = 0; w < e->W; ++w) e->mask.w[w] = state_mask != nullptr ? state_mask[w] : 0ULL;
     const int bps = cfg->blocks_per_sm > 0 ? std::min(cfg->blocks_per_sm, kSweepBlocksPerSM) : kSweepBlocksPerSM;
-    e->grid = sms * bps; // one resident wave of the sweep
+    e->grid = std::min(sms * bps, kMaxGrid); // one resident wave of the sweep (the resolve keeps a prefix per block)
     e->table_shift = cfg->table_shift > 0 ? std::min(cfg->table_shift, 3) : 1;
     mpx_engine *eng = e;
     auto bail = [&](mpx_status st) {
@@ -1696,23 +1787,41 @@ mpx_status create_engine(const mpx_config *cfg, const uint64_t *obs_words, const
     if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_partial), e->grid * sizeof(double));
     if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_out), sizeof(double));
     if (ce == cudaSuccess) ce = pinned_get(reinterpret_cast<void **>(&e->h_out), sizeof(double));
-    if (ce == cudaSuccess && n_obs > 0) {
-        ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_keys), n_obs * e->W * sizeof(uint64_t));
-        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_coef), n_obs * sizeof(double));
+    if (ce == cudaSuccess && n_init_terms > 0) {
+        ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_keys), n_init_terms * e->W * sizeof(uint64_t));
         if (ce == cudaSuccess)
-            ce = cudaMemcpyAsync(e->d_init_keys, obs_words, n_obs * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice,
+            ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_init_coef), n_init_terms * sizeof(double));
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(e->d_init_keys, init_words, n_init_terms * e->W * sizeof(uint64_t),
+                                 cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(e->d_init_coef, init_coef, n_init_terms * sizeof(double), cudaMemcpyHostToDevice,
                                  e->stream);
-        if (ce == cudaSuccess)
-            ce = cudaMemcpyAsync(e->d_init_coef, obs_coef, n_obs * sizeof(double), cudaMemcpyHostToDevice, e->stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream); // the caller's arrays may go away
     }
+    if (ce == cudaSuccess && cfg->has_schrodinger) {
+        // the observable, for <O> = core + observable . state
+        e->schr = true;
+        e->tr.schr = 1;
+        e->tr.occ = e->mask;
+        e->n_obs = n_obs;
+        const uint64_t k = std::max<uint64_t>(n_obs, 1);
+        ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_keys), k * e->W * sizeof(uint64_t));
+        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_coef), k * sizeof(double));
+        if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_idx), k * sizeof(uint32_t));
+        if (ce == cudaSuccess && n_obs > 0)
+            ce = cudaMemcpyAsync(e->d_obs_keys, obs_words, n_obs * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                 e->stream);
+        if (ce == cudaSuccess && n_obs > 0)
+            ce = cudaMemcpyAsync(e->d_obs_coef, obs_coef, n_obs * sizeof(double), cudaMemcpyHostToDevice, e->stream);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream); // the caller's arrays may go away
     if (ce != cudaSuccess) {
         e->err = std::string("CUDA setup failed: ") + cudaGetErrorString(ce);
         cudaGetLastError();
         return bail(MPX_ERR_CUDA);
     }
-    e->n_init = n_obs;
-    const uint64_t cap = std::max<uint64_t>({cfg->capacity_hint, 4 * n_obs, 4096});
+    e->n_init = n_init_terms;
+    const uint64_t cap = std::max<uint64_t>({cfg->capacity_hint, 4 * n_init_terms, 4096});
     s = alloc_store(eng, cap, 0);
     if (s != MPX_OK) return bail(s);
     s = load_initial(eng);
@@ -1769,8 +1878,8 @@ mpx_status mpx_circuit_set_angles(mpx_engine *e, mpx_circuit *c, const double *a
     if (e == nullptr || c == nullptr || (c->n > 0 && angles == nullptr)) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
-    std::vector<GateDesc> h(c->n);
-    for (uint64_t l = 0; l < c->n; ++l) make_desc(e, c->words.data() + l * e->W, angles[l], h[l]);
+    std::vector<GateDesc> h;
+    make_descs(e, c->words.data(), angles, c->n, h);
     c->any_cos_zero = false;
     for (const GateDesc &g : h) c->any_cos_zero = c->any_cos_zero || g.cos_zero;
     c->angles.assign(angles, angles + c->n);
@@ -1805,9 +1914,20 @@ mpx_status mpx_expectation(mpx_engine *e, double *out) {
     if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     MPX_CUDA(cudaSetDevice(e->device));
-    pick_exp(e->W, e->cfg.basis)(e);
-    k_expect_final<<<1, 32, 0, e->stream>>>(e->d_partial, static_cast<uint32_t>(e->grid), e->core, e->d_out);
-    e->launches += 2;
+    if (e->schr) {
+        // Schrodinger: core + observable . state (MPFunctions.cpp:196-205), each observable term looked up
+        uint64_t n_live = 0;
+        mpx_status s = mpx_size(e, &n_live);
+        if (s != MPX_OK) return s;
+        if (e->n_obs > 0) pick_lookup(e->W)(e, e->d_obs_keys, e->n_obs, n_live, e->d_obs_idx);
+        k_expect_schr<<<1, kBlock, 0, e->stream>>>(e->d_obs_idx, e->d_obs_coef, e->n_obs, e->st.coef, e->core, e->d_out);
+        e->launches += e->n_obs > 0 ? 2 : 1;
+    }
+    else {
+        pick_exp(e->W, e->cfg.basis)(e);
+        k_expect_final<<<1, 32, 0, e->stream>>>(e->d_partial, static_cast<uint32_t>(e->grid), e->core, e->d_out);
+        e->launches += 2;
+    }
     MPX_CUDA(cudaGetLastError());
     MPX_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     MPX_CUDA(cudaStreamSynchronize(e->stream));
@@ -1996,6 +2116,9 @@ mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t seg
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
     if (e->tr.has_len_k)
         return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
+    if (e->schr)
+        return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
+                                        "the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = adjoint_forward(e, *c, segment_gates);
     if (s != MPX_OK) return s;
@@ -2027,6 +2150,9 @@ mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
     if (e->tr.has_len_k)
         return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
+    if (e->schr)
+        return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
+                                        "the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = graph_build(e, *c, segment_gates);
     if (s != MPX_OK) return s;
@@ -2123,6 +2249,29 @@ mpx_status mpx_update_initial_operator(mpx_engine *e, const uint64_t *words, con
     if (e == nullptr || (n > 0 && (words == nullptr || coefs == nullptr))) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     MPX_CUDA(cudaSetDevice(e->device));
+    if (e->schr) {
+        // Schrodinger: the observable is dotted into the evolved state, so re-weighting it replaces the
+        // observable's terms (a term the state does not hold contributes 0)
+        if (n > std::max<uint64_t>(e->n_obs, 1)) {
+            dev_free(e, e->d_obs_keys);
+            dev_free(e, e->d_obs_coef);
+            dev_free(e, e->d_obs_idx);
+            e->d_obs_keys = nullptr;
+            e->d_obs_coef = nullptr;
+            e->d_obs_idx = nullptr;
+            MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_keys), n * e->W * sizeof(uint64_t)));
+            MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_coef), n * sizeof(double)));
+            MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->d_obs_idx), n * sizeof(uint32_t)));
+        }
+        if (n > 0) {
+            MPX_CUDA(cudaMemcpyAsync(e->d_obs_keys, words, n * e->W * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream));
+            MPX_CUDA(cudaMemcpyAsync(e->d_obs_coef, coefs, n * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        }
+        e->n_obs = n;
+        if (has_core) e->core = core;
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+        return MPX_OK;
+    }
     uint64_t n_live = 0;
     mpx_status s = mpx_size(e, &n_live);
     if (s != MPX_OK) return s;
@@ -2337,15 +2486,19 @@ mpx_status mpx_clone(mpx_engine *e, const mpx_circuit *c, mpx_engine **out, mpx_
     MPX_CUDA(cudaSetDevice(e->device));
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     const int W = e->W;
-    std::vector<uint64_t> ik(std::max<uint64_t>(e->n_init, 1) * W);
-    std::vector<double> ic(std::max<uint64_t>(e->n_init, 1));
-    if (e->n_init > 0) {
-        MPX_CUDA(cudaMemcpy(ik.data(), e->d_init_keys, e->n_init * W * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-        MPX_CUDA(cudaMemcpy(ic.data(), e->d_init_coef, e->n_init * sizeof(double), cudaMemcpyDeviceToHost));
+    // the observable the engine was created with (Schrodinger: kept apart from the store)
+    const uint64_t n_o = e->schr ? e->n_obs : e->n_init;
+    const uint64_t *d_ok = e->schr ? e->d_obs_keys : e->d_init_keys;
+    const double *d_oc = e->schr ? e->d_obs_coef : e->d_init_coef;
+    std::vector<uint64_t> ik(std::max<uint64_t>(n_o, 1) * W);
+    std::vector<double> ic(std::max<uint64_t>(n_o, 1));
+    if (n_o > 0) {
+        MPX_CUDA(cudaMemcpy(ik.data(), d_ok, n_o * W * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        MPX_CUDA(cudaMemcpy(ic.data(), d_oc, n_o * sizeof(double), cudaMemcpyDeviceToHost));
     }
     mpx_engine *d = nullptr;
-    mpx_status s = create_engine(&e->cfg, e->n_init > 0 ? ik.data() : nullptr, e->n_init > 0 ? ic.data() : nullptr,
-                                 e->n_init, e->core, e->mask.w, &d, !e->keep_blocks);
+    mpx_status s = create_engine(&e->cfg, n_o > 0 ? ik.data() : nullptr, n_o > 0 ? ic.data() : nullptr, n_o, e->core,
+                                 e->mask.w, &d, !e->keep_blocks);
     if (s != MPX_OK) return fail(eng, s, mpx_last_error(nullptr));
     s = clone_into(e, d);
     if (s == MPX_OK && c != nullptr) {
@@ -2411,6 +2564,9 @@ void mpx_destroy(mpx_engine *e) {
     dev_free(e, e->d_basis);
     dev_free(e, e->d_stats);
     clear_start(e);
+    dev_free(e, e->d_obs_keys);
+    dev_free(e, e->d_obs_coef);
+    dev_free(e, e->d_obs_idx);
     if (e->stream != nullptr) {
         cudaStreamSynchronize(e->stream); // the pool frees above are stream-ordered
         cudaStreamDestroy(e->stream);

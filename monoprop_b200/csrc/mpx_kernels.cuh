@@ -485,40 +485,79 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
     }
 }
 
+constexpr int kMaxGrid = 1024; // largest per-gate grid (148 SMs x at most 4 blocks per SM, with headroom)
+
 // Partner resolve + rotation apply + append (Engine.h:364-513, FusedApply.h:32-83, MPOperator.h:269-278).
-// Resolve block b processes the query region of sweep block b, in block-wide rounds; appends
-// take one counter bump per round. In REPLAY mode the keys of this gate's appends already exist
-// (indices >= n0, inserted by the forward pass): a partner found there is treated as the append it was,
-// nothing is inserted, and every rotated or appended pair goes to the tape's pair log with both
-// pre-gate coefficients (one counter bump per round).
+// The sweep leaves the emitted branches of a gate in per-sweep-block query regions of very uneven fill
+// (anticommuting terms cluster in index ranges, so a few blocks hold most of them). Every resolve block
+// therefore first forms the exclusive prefix of the regions' counts in shared memory and takes an equal
+// contiguous share of the gate's queries, whichever regions they lie in; a query's region is found by a
+// binary search over the prefix. The block works through its share in block-wide rounds, one query per
+// thread; appends take one counter bump per round. In REPLAY mode the keys of this gate's appends
+// already exist (indices >= n0, inserted by the forward pass): a partner found there is treated as the
+// append it was, nothing is inserted, and every rotated or appended pair goes to the tape's pair log with
+// both pre-gate coefficients (one counter bump per round).
 template <int W, int BASIS, bool REPLAY = false, bool LENK = false>
 __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                      Trunc tr, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
     __shared__ unsigned long long s_base, s_rbase;
+    __shared__ uint32_t s_pfx[kMaxGrid + 1]; // exclusive prefix of the regions' query counts
+    __shared__ uint32_t s_wsum[kWarps];
     pdl_trigger();
-    // the gate (constant circuit data) before the dependency wait; counters and query count after it
+    // the gate (constant circuit data) before the dependency wait; counters and query counts after it
     const GateDesc &gd = gates[gate];
     const bool empty = gd.empty != 0;
     pdl_wait();
     const uint32_t stall = cnt->stall;
     const uint64_t n0 = cnt->n0;
-    const uint32_t total = sc.blk_q[blockIdx.x];
     if (stall != kNoStall) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const SweepGeometry geo = sweep_geometry(n0);
     if (empty || n0 == 0) return;
-    if (total == 0) return;
-    const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
+    // prefix of the per-region counts: thread t owns regions [t*per, (t+1)*per)
+    const uint32_t G = gridDim.x;
+    const uint32_t per = (G + kBlock - 1) / kBlock;
+    uint32_t mine = 0;
+    for (uint32_t r = threadIdx.x * per; r < (threadIdx.x + 1) * per && r < G; ++r) mine += sc.blk_q[r];
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) wbase += (w < warp) ? s_wsum[w] : 0u;
+    {
+        uint32_t acc = wbase + incl - mine;
+        for (uint32_t r = threadIdx.x * per; r < (threadIdx.x + 1) * per && r < G; ++r) {
+            s_pfx[r] = acc;
+            acc += sc.blk_q[r];
+        }
+    }
+    uint32_t Q = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) Q += s_wsum[w];
+    if (threadIdx.x == 0) s_pfx[G] = Q;
+    __syncthreads();
+    if (Q == 0) return;
+    // this block's equal share [lo, hi) of the gate's Q queries
+    const uint32_t lo = static_cast<uint32_t>((static_cast<uint64_t>(Q) * blockIdx.x) / G);
+    const uint32_t hi = static_cast<uint32_t>((static_cast<uint64_t>(Q) * (blockIdx.x + 1)) / G);
+    if (lo == hi) return;
+    const uint64_t region_slots = static_cast<uint64_t>(kWarps) * geo.stride;
     uint64_t g[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) g[w] = gd.g[w];
     const double sinv = gd.sinv, inv_cos = gd.inv_cos;
     const bool cos_zero = gd.cos_zero != 0;
 
-    for (uint32_t tb = 0; tb < total; tb += kBlock) {
+    for (uint32_t tb = lo; tb < hi; tb += kBlock) { // block-uniform rounds
         const uint32_t k = tb + threadIdx.x;
         bool miss = false, rec = false;
         uint64_t p[W];
@@ -526,8 +565,15 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
         uint32_t tag = 0, src = 0, tgt = 0;
         int8_t code = 0;
         double v = 0.0, ph = 0.0, vt = 0.0;
-        if (k < total) {
-            const uint64_t q = qbase + k;
+        if (k < hi) {
+            // region of query k: the last r with s_pfx[r] <= k
+            uint32_t a = 0, b = G;
+            while (b - a > 1) {
+                const uint32_t mid = (a + b) >> 1;
+                if (s_pfx[mid] <= k) a = mid;
+                else b = mid;
+            }
+            const uint64_t q = a * region_slots + (k - s_pfx[a]);
             src = sc.q_src[q];
             const uint8_t flag = sc.q_flag[q];
             v = sc.q_val[q];
@@ -628,7 +674,16 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
         else if (miss) {
             const uint64_t idx = s_base + off + __popc(ball & lt_mask);
             store_key<W>(st.keys, idx, p);
-            st.coef[idx] = (sinv * ph) * v;
+            double c_new = (sinv * ph) * v; // Heisenberg: the new term starts from 0
+            if (tr.schr) {
+                // Schrodinger (FusedApply.h:39-83): the new slot starts from its reference-state score vt,
+                // and the pair rotates as a hit does (the source's cos factor is already applied)
+                const double vt0 = state_score<W, BASIS>(p, tr.occ);
+                st.coef[src] = __fma_rn(sinv * -ph, vt0, st.coef[src]);
+                c_new = (!cos_zero && !LENK) ? __fma_rn(gd.cosv, vt0, (sinv * ph) * v)
+                                             : __fma_rn(sinv * ph, v, gd.cosv * vt0);
+            }
+            st.coef[idx] = c_new;
             const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
             for (uint64_t probes = 0;; ++probes) {
                 if (probes > st.tmask) {
@@ -819,6 +874,23 @@ __global__ void k_lookup(Store st, const uint64_t *__restrict__ qkeys, uint64_t 
         }
         out[q] = found;
     }
+}
+
+// Schrodinger picture: <O> = core + sum_t obs_coef[t] * state[idx[t]], the observable dotted into the evolved
+// state (MPFunctions.cpp:196-205); idx[t] = kNoStall for a term the state does not hold (contributes 0).
+// One block, fixed summation order.
+__global__ void __launch_bounds__(kBlock) k_expect_schr(const uint32_t *__restrict__ idx,
+                                                         const double *__restrict__ obs_coef, uint64_t n_obs,
+                                                         const double *__restrict__ coef, double core,
+                                                         double *__restrict__ out) {
+    __shared__ double s_red[kBlock / 32];
+    double acc = 0.0;
+    for (uint64_t t = threadIdx.x; t < n_obs; t += kBlock) {
+        const uint32_t j = idx[t];
+        if (j != kNoStall) acc += obs_coef[t] * coef[j];
+    }
+    const double total = block_sum(acc, s_red);
+    if (threadIdx.x == 0) out[0] = core + total;
 }
 
 // coef[idx[k]] = val[k] (indices distinct).

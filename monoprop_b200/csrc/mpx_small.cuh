@@ -199,7 +199,14 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
                 const uint32_t idx = atomicAdd(&s_n, 1u);
 #pragma unroll
                 for (int w = 0; w < W; ++w) keys[idx * W + w] = p[w];
-                coef[idx] = (sinv * ph) * v;
+                if (tr.schr) { // Schrodinger: the new slot starts from its reference-state score
+                    const double vt0 = state_score<W, BASIS>(p, tr.occ);
+                    coef[src] = __fma_rn(sinv * -ph, vt0, coef[src]);
+                    coef[idx] = __fma_rn(cosv, vt0, (sinv * ph) * v);
+                }
+                else {
+                    coef[idx] = (sinv * ph) * v;
+                }
                 small_insert<W>(table, tmask, keys, idx, cnt);
             }
         }

@@ -196,7 +196,7 @@ class MonomialPropagator:
 
     @property
     def schrodinger(self) -> bool:
-        return False
+        return self._simulator.schrodinger
 
     @staticmethod
     def _bind(parameters) -> list[float]:
