@@ -210,6 +210,12 @@ def main() -> None:
                     help="profiling case instead of the benchmark: a store of this many random 100-qubit terms of "
                          "Pauli weight <= 10, then the last --case-gates gates of the 10x10 circuit")
     ap.add_argument("--case-gates", type=int, default=4)
+    ap.add_argument("--regime-case", type=int, default=0,
+                    help="profiling case in the benchmark's own regime: the 10x10 circuit propagated until the store "
+                         "holds this many terms, then --case-gates more gates inside the NVTX range mpx_profile")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="profiling case for the other kernels (shared-memory path, expectation, columns, table "
+                         "build, frozen replay and adjoint), each inside an NVTX range named after it")
     ap.add_argument("--no-gradient", action="store_true", help="skip the <O> + full-gradient measurement")
     ap.add_argument("--no-sub-results", action="store_true",
                     help="skip the compact measurements of the 20-qubit line and 6x6 Hubbard circuits")
@@ -218,6 +224,12 @@ def main() -> None:
     args = ap.parse_args()
     if args.kernel_case:
         kernel_case(args.kernel_case, args.case_gates)
+        return
+    if args.regime_case:
+        regime_case(args.regime_case, args.case_gates)
+        return
+    if args.profile_kernels:
+        profile_kernels()
         return
     if args.workload == "batch":
         batch_bench(args)
@@ -311,8 +323,10 @@ def main() -> None:
     torch.cuda.synchronize()
     ms = []
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("bench_step")  # what a kernel profiler selects for the launch list
         for _ in range(args.steps):
             ms.append(one_step(False))
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -617,6 +631,90 @@ def kernel_case(n_terms: int, n_gates: int) -> None:
     st = eng.gate_stats()
     print(json.dumps({"kernel_case_terms": int(keys.shape[0]), "n_g": st.n.tolist(), "a_g": st.anti.tolist(),
                       "e_g": st.emitted.tolist(), "m_g": st.appended.tolist()}), flush=True)
+    eng.close()
+
+
+def regime_case(n_terms: int, n_gates: int) -> None:
+    """The 100-qubit benchmark circuit in its own regime: propagated (gates last to first) until the store
+    holds about ``n_terms`` terms, then ``n_gates`` more gates inside the NVTX range ``mpx_profile`` (what a
+    kernel profiler selects)."""
+    import torch
+
+    from monoprop_b200 import _native
+    from monoprop_b200 import workloads as WL
+
+    wl = WL.ising100()
+    gw, ang = wl.gen_words(), wl.angles()
+    L = wl.n_layers
+    eng = _native.engine_for(wl)
+    eng.propagate(gw, ang)
+    n = eng.gate_stats().n
+    eng.close()
+    _native.load().mpx_trim_device_memory(0)  # hand the full-size store back before the profiled case
+    steps = int(np.searchsorted(n, n_terms))  # applied steps before the profiled gates
+    steps = min(steps, L - n_gates)
+    eng = _native.engine_for(wl)
+    eng.propagate(gw[L - steps:], ang[L - steps:])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("mpx_profile")
+    eng.propagate(gw[L - steps - n_gates:L - steps], ang[L - steps - n_gates:L - steps])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    st = eng.gate_stats()
+    print(json.dumps({"regime_case_steps_before": steps, "n_g": st.n.tolist(), "a_g": st.anti.tolist(),
+                      "e_g": st.emitted.tolist(), "m_g": st.appended.tolist()}), flush=True)
+    eng.close()
+
+
+def profile_kernels() -> None:
+    """Small cases for the kernels the benchmark step does not profile: the shared-memory path (the
+    20-qubit line circuit), the expectation reduction, the column and table builds (the 100-qubit circuit's
+    first 1200 gates, with a reset), and the frozen replay and adjoint kernels (its gradient with
+    checkpoints every 280 gates), each inside an NVTX range named after the work."""
+    import torch
+
+    from monoprop_b200 import _native
+    from monoprop_b200 import workloads as WL
+
+    nvtx = torch.cuda.nvtx
+    wl = WL.line20()
+    eng = _native.engine_for(wl)
+    torch.cuda.synchronize()
+    nvtx.range_push("small_path")
+    eng.propagate(wl.gen_words(), wl.angles())
+    torch.cuda.synchronize()
+    nvtx.range_pop()
+    eng.close()
+    wl = WL.ising100()
+    L = 1200
+    gw, ang = wl.gen_words()[:L], wl.angles()[:L]
+    eng = _native.engine_for(wl)
+    circ = eng.upload(gw, ang)
+    eng.propagate_circuit(circ)
+    torch.cuda.synchronize()
+    nvtx.range_push("expectation")
+    eng.expectation()
+    torch.cuda.synchronize()
+    nvtx.range_pop()
+    nvtx.range_push("reset_build")
+    eng.reset()
+    torch.cuda.synchronize()
+    nvtx.range_pop()
+    ev = eng.adjoint_forward(circ, 280)
+    torch.cuda.synchronize()
+    nvtx.range_push("adjoint_backward")
+    g = eng.adjoint_backward(circ)
+    torch.cuda.synchronize()
+    nvtx.range_pop()
+    eng.graph_build(circ)
+    torch.cuda.synchronize()
+    nvtx.range_push("frozen_replay")
+    eng.graph_expectation(circ)
+    torch.cuda.synchronize()
+    nvtx.range_pop()
+    print(json.dumps({"profile_kernels": "ok", "terms": eng.size(), "expectation": ev,
+                      "grad_abs_max": float(np.max(np.abs(g)))}), flush=True)
+    circ.close()
     eng.close()
 
 

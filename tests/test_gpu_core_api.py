@@ -136,8 +136,8 @@ def test_update_initial_operator_after_propagate():
     p.propagate([list(m) for m in wl.gate_slots], list(map(int, wl.param_map)), list(wl.gen_coeffs),
                 list(wl.params), None)
     terms = p.evolved_operator([], 0.0)
-    zonly = [k for k in terms if len(k) and all(k[i] // 2 == k[i + 1] // 2 for i in range(0, len(k), 2))
-             and len(k) % 2 == 0][:5]
+    zonly = [k for k in terms if len(k) and len(k) % 2 == 0
+             and all(k[i] % 2 == 0 and k[i + 1] == k[i] + 1 for i in range(0, len(k), 2))][:5]
     other = [k for k in terms if len(k) and k not in zonly][:5]
     new = {**{k: 0.1 * (i + 1) + 0j for i, k in enumerate(zonly)}, **{k: 7.0 + 0j for k in other}, (): 0.5 + 0j}
     p.update_initial_operator(new)

@@ -80,7 +80,9 @@ def test_core_schrodinger_surface():
                 list(wl.params[:P]), None)
     ev = p.expectation_value([])
     assert abs(ev - float(g["expectation"])) <= 1e-10 * max(1.0, abs(float(g["expectation"])))
-    assert () not in p.evolved_operator([], 0.0)
+    # the state's identity monomial (score 1, never rotated) is a stored term; the observable's core term is
+    # not added in this picture (binder.h:200-221)
+    assert p.evolved_operator([], 0.0)[()] == 1.0
     # <O> is linear in the observable: doubling its non-core part doubles <O> - core
     p.update_initial_operator({(): 0.5 + 0j, (0, 1): 1.0j})
     assert abs((p.expectation_value([]) - 0.5) - 2 * (ev - 0.5)) <= 1e-12
