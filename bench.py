@@ -525,7 +525,7 @@ def batch_bench(args) -> None:
     import torch
 
     from monoprop_b200 import workloads as WL
-    from monoprop_b200.batch import Autotuner, BatchConfig, run_batch
+    from monoprop_b200.batch import Autotuner, BatchConfig, run_batch, shard_instances
 
     rank, world, local, dist = _dist()
     torch.cuda.set_device(local)
@@ -535,8 +535,8 @@ def batch_bench(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     full = WL.batch_ising50(args.batch_instances)
-    # instances are independent: rank r takes every world-th one (no data-path collective)
-    batch = full[rank::world]
+    # instances are independent: rank r takes its deepest-first round-robin share (no data-path collective)
+    batch = [full[i] for i in shard_instances(full, rank, world)]
     seg = 4 * 135
     run_batch(batch[-4:], BatchConfig(), gradient=True, segment_gates=seg, device=local)  # warm-up
     tuner = Autotuner(cache_path=os.path.join(tempfile.gettempdir(), f"mpx_autotune_{os.getpid()}.json"))

@@ -118,6 +118,14 @@ def run_batch(workloads, config: BatchConfig | None = None, gradient: bool = Fal
     return BatchResult(ev, grads, terms, dt, exports)
 
 
+def shard_instances(workloads, rank: int, world: int) -> list[int]:
+    """Indices of the instances rank ``rank`` of ``world`` propagates when a batch is split over GPUs (no
+    data-path collective: instances are independent). Instances are dealt deepest first, round robin, so
+    every rank gets a near-equal number of gates: the ranks' totals differ by at most one instance depth."""
+    order = sorted(range(len(workloads)), key=lambda i: (-workloads[i].n_layers, i))
+    return order[rank::world]
+
+
 def signature(workloads) -> str:
     """Workload family key for the tuning cache: basis, key width, truncation, size of the batch."""
     w0 = workloads[0]

@@ -45,6 +45,42 @@ def test_max_over_ranks_two_gloo_ranks():
     assert out[0] == out[1] == 11.0
 
 
+def _shard_main(rank, world, port, out):
+    import torch.distributed as dist
+
+    from monoprop_b200.batch import shard_instances
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    full = W.batch_ising50(40, seed=4)
+    mine = shard_instances(full, rank, world)
+    got = [None] * world
+    dist.all_gather_object(got, mine)
+    out[rank] = got
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_batch_instance_split_two_gloo_ranks():
+    """The multi-GPU batch split (bench.py --workload batch under torchrun): two ranks take disjoint
+    shares that cover every instance once, with gate totals within one instance depth of each other."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    shares = out[0]
+    assert out[1] == shares
+    full = W.batch_ising50(40, seed=4)
+    assert sorted(shares[0] + shares[1]) == list(range(40)) and not set(shares[0]) & set(shares[1])
+    gates = [sum(full[i].n_layers for i in s) for s in shares]
+    assert abs(gates[0] - gates[1]) <= max(wl.n_layers for wl in full)
+
+
 def test_batch_run_rejects_null_buffers_without_touching_a_device():
     lib = _native.load()
     cfg = _native.Config(1, 1, 4, 0, 0.0, 0, 0.0, 8, 0, 0, 0, 0)
