@@ -130,11 +130,12 @@ MPX_API mpx_status mpx_set_cutoff_type(mpx_engine *e, int32_t cutoff_type);
 MPX_API mpx_status mpx_set_lower_atol(mpx_engine *e, int32_t has_value, double value);
 MPX_API mpx_status mpx_set_upper_atol(mpx_engine *e, int32_t has_value, double value);
 
-/* only_rotate_len_k of the next propagate calls (MonomialPropagator::propagate's argument,
- * MonomialPropagator.inl:696-718; semantics Scan.h:146-157,376-391 and FusedApply.h:46-52): a term with
- * more than k set slots takes no part in a gate (neither cos-scaled nor emitted), and a partner outside
- * that set receives its sine term unscaled. k <= 0 clears it; k > 2*num_modes is rejected with the
- * reference's message. The gradient and graph entry points reject an engine with k set. */
+/* only_rotate_len_k of the next propagate, gradient forward or graph build calls (the argument of
+ * MonomialPropagator::propagate and ::build_graph, MonomialPropagator.inl:696-718, binder.h:102-110;
+ * semantics Scan.h:146-157,376-391 and FusedApply.h:46-52): a term with more than k set slots takes no
+ * part in a gate (neither cos-scaled nor emitted), and a partner outside that set receives its sine term
+ * unscaled. A gradient or graph keeps the k it was recorded with. k <= 0 clears it; k > 2*num_modes is
+ * rejected with the reference's message. */
 MPX_API mpx_status mpx_set_only_rotate_len_k(mpx_engine *e, int64_t k);
 
 /* basis_change of a Majorana engine (the constructor argument, MonomialPropagator.inl:82-131,460-495):

@@ -259,7 +259,10 @@ public:
                      std::optional<std::vector<double>> parameters, std::optional<unsigned int> only_rotate_len_k) {
         if (!parameters.has_value())
             throw NotSupported("build_graph without seed parameters (a purely structural graph) is not implemented");
-        if (only_rotate_len_k.has_value()) throw NotSupported("only_rotate_len_k: not implemented by the B200 engine");
+        // validate_only_rotate_len_k_ (Validation.cpp:119-128), as propagate
+        if (only_rotate_len_k.has_value() && (*only_rotate_len_k == 0 || *only_rotate_len_k > 2 * logical_))
+            throw PropagatorConfigError("only_rotate_len_k=" + std::to_string(*only_rotate_len_k) +
+                                        " is out of range; must be 0 < k <= 2*num_qubits");
         std::vector<uint64_t> words;
         std::vector<double> angles;
         encode_circuit(majoranas, parameter_mapping, gen_coeffs, *parameters, words, angles);
@@ -280,11 +283,13 @@ public:
         }
         ++graph_epoch_;
         double ev = 0.0;
-        mpx_status st;
-        {
+        mpx_status st = mpx_set_only_rotate_len_k(
+            e_, only_rotate_len_k.has_value() ? static_cast<int64_t>(*only_rotate_len_k) : 0);
+        if (st == MPX_OK) {
             py::gil_scoped_release nogil;
-            st = mpx_graph_build(e_, circ_, 0, &ev);
+            st = mpx_graph_build(e_, circ_, 0, &ev); // the graph keeps the k it was built with
         }
+        mpx_set_only_rotate_len_k(e_, 0);
         if (st != MPX_OK) { // no graph is kept after a failed build
             const std::string msg = mpx_last_error(e_);
             mpx_circuit_destroy(circ_);

@@ -161,6 +161,16 @@ __global__ void __launch_bounds__(kBlock) k_adj_pairs(Tape tp, const GateDesc *_
             const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
             const double vs = tp.p_vs[r], vt = tp.p_vt[r];
             const double ls = lam[s], lt = lam[t];
+            if (code & 0x20) {
+                // partner outside the only_rotate_len_k set: c_T' = c_T + s phi c_S (no cos factor), so
+                // d(c_T')/dangle = 2 C phi v_S and lambda_T = lambda_T' - s phi lambda_S'; T is not in the
+                // undo log (it is not scaled by this gate), so it takes no done bit
+                acc += ls * (-2.0 * S * vs - 2.0 * C * phi * vt) + lt * (2.0 * C * phi * vs);
+                lam[s] = C * ls + S * phi * lt;
+                lam[t] = lt - S * phi * ls;
+                atomicOr(&done[s >> 5], 1u << (s & 31));
+                continue;
+            }
             // d(c_S')/dangle = -2 s v_S - 2 C phi v_T;  d(c_T')/dangle = -2 s v_T + 2 C phi v_S
             acc += ls * (-2.0 * S * vs - 2.0 * C * phi * vt) + lt * (-2.0 * S * vt + 2.0 * C * phi * vs);
             lam[s] = C * ls + S * phi * lt;
@@ -198,7 +208,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__
             const uint64_t r = base + k;
             const uint32_t i = tp.u_idx[r];
             const uint32_t bit = 1u << (i & 31);
-            if (done[i >> 5] & bit) {
+            if (i == kNoStall) {
+                // an anticommuting term outside the only_rotate_len_k set: untouched by the gate
+            }
+            else if (done[i >> 5] & bit) {
                 atomicAnd(&done[i >> 5], ~bit);
             }
             else {
@@ -249,6 +262,8 @@ struct Frozen {
     // (-1: never); a step skips the cos scaling of a term with last < step and the rotation of a pair with
     // both endpoints below it. nullptr: no paring.
     const int32_t *last;
+    // only_rotate_len_k of the build: one bit per term of more than k slots (never cos-scaled); nullptr: none
+    const uint32_t *longb;
 };
 
 // ----- paring ---------------------------------------------------------------------------------------------
@@ -313,12 +328,13 @@ __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ co
         const double vs = coef[s], vt = appended ? 0.0 : coef[t];
         const bool pared = fz.last != nullptr && fz.last[s] < static_cast<int32_t>(step) &&
                            fz.last[t] < static_cast<int32_t>(step);
+        const bool unscaled_t = (code & 0x20) != 0; // partner outside the only_rotate_len_k set
         if (!pared) {
             coef[s] = C * vs - S * phi * vt;
-            coef[t] = C * vt + S * phi * vs;
+            coef[t] = (unscaled_t ? vt : C * vt) + S * phi * vs;
         }
         atomicOr(&done[s >> 5], 1u << (s & 31));
-        if (!appended) atomicOr(&done[t >> 5], 1u << (t & 31));
+        if (!appended && !unscaled_t) atomicOr(&done[t >> 5], 1u << (t & 31));
         if constexpr (LOG) {
             const uint64_t r = tp.p_base[step] + k;
             tp.p_src[r] = s;

@@ -64,6 +64,9 @@ struct AdjointState {
     uint64_t *r_begin = nullptr;
     uint64_t r_total = 0;
     bool rec_ok = false;
+    // only_rotate_len_k of the forward pass (0: none) and its outside-set bits over the final store
+    uint32_t len_k = 0;
+    uint32_t *longb = nullptr;
 };
 
 // A frozen structure (the surrogate "graph" of the reference's variational loop): every gate's rotated
@@ -81,7 +84,8 @@ struct FrozenGraph {
     bool pared = false;                     // the frozen kernels skip pared terms
     double last_for = -1.0;                 // threshold `last` was computed for (< 0: none yet)
     // the device view the frozen kernels take
-    Frozen view() const { return Frozen{src, tgt, code, p_begin, p_count, pared ? last : nullptr}; }
+    uint32_t *longb = nullptr;              // only_rotate_len_k of the build: terms outside its set (bits)
+    Frozen view() const { return Frozen{src, tgt, code, p_begin, p_count, pared ? last : nullptr, longb}; }
 };
 
 struct mpx_engine {
@@ -422,21 +426,30 @@ void launch_gate(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t 
     }
 }
 
-// A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends. (The
-// gradient rejects only_rotate_len_k; basis_change changes only the emit decisions, replayed alike.)
+template <int W, int B, int EXT>
+void launch_replay_ext(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
+    launch_dep(e, &k_sweep<W, B, true, EXT>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp, e->d_stats);
+    launch_dep(e, &k_resolve<W, B, true, (EXT & 1) != 0>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
+    launch_dep_on(e, 1, 32, &k_replay_advance, e->d_cnt, tp.n_next, step);
+}
+
+// A gate replayed for the gradient: same sweep and resolve, logging to the tape; no appends. The variant
+// follows the engine's options (only_rotate_len_k; basis_change, which changes only the emit decisions).
 template <int W, int B>
 void launch_replay(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, const Tape &tp) {
-    bool mapped = false;
+    const int ext = (e->tr.has_len_k ? 1 : 0) | (B == 0 && e->tr.basis_rows != nullptr ? 2 : 0);
     if constexpr (B == 0) {
-        if (e->tr.basis_rows != nullptr) {
-            launch_dep(e, &k_sweep<W, B, true, 2>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp, e->d_stats);
-            mapped = true;
+        switch (ext) {
+        case 0: launch_replay_ext<W, B, 0>(e, d_desc, gate, step, tp); break;
+        case 1: launch_replay_ext<W, B, 1>(e, d_desc, gate, step, tp); break;
+        case 2: launch_replay_ext<W, B, 2>(e, d_desc, gate, step, tp); break;
+        default: launch_replay_ext<W, B, 3>(e, d_desc, gate, step, tp); break;
         }
     }
-    if (!mapped)
-        launch_dep(e, &k_sweep<W, B, true>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp, e->d_stats);
-    launch_dep(e, &k_resolve<W, B, true>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, tp);
-    launch_dep_on(e, 1, 32, &k_replay_advance, e->d_cnt, tp.n_next, step);
+    else {
+        if (ext & 1) launch_replay_ext<W, B, 1>(e, d_desc, gate, step, tp);
+        else launch_replay_ext<W, B, 0>(e, d_desc, gate, step, tp);
+    }
 }
 
 // Shared-memory capacity of the single-block path per key width: the largest power-of-two-friendly size
@@ -475,7 +488,7 @@ template <int W, bool LOG>
 void launch_frozen(mpx_engine *e, const GateDesc *d_desc, const Frozen &fz, uint32_t gate, uint32_t step, uint64_t n0,
                    uint32_t *done, const Tape &tp) {
     launch_dep(e, &k_frozen_pairs<LOG>, e->st.coef, fz, d_desc, gate, step, done, tp);
-    launch_dep(e, &k_frozen_scan<W, LOG>, e->st, d_desc, gate, step, n0, done, tp, fz.last);
+    launch_dep(e, &k_frozen_scan<W, LOG>, e->st, d_desc, gate, step, n0, done, tp, fz.last, fz.longb);
 }
 
 using FrozenFn = void (*)(mpx_engine *, const GateDesc *, const Frozen &, uint32_t, uint32_t, uint64_t, uint32_t *,
@@ -610,6 +623,24 @@ LookupFn pick_lookup(int W) {
     case 6: return &launch_lookup<6>;
     case 7: return &launch_lookup<7>;
     default: return &launch_lookup<8>;
+    }
+}
+
+template <int W>
+void launch_long_bits(mpx_engine *e, uint64_t n, uint32_t len_k, uint32_t *out, unsigned blocks) {
+    k_long_bits<W><<<blocks, 256, 0, e->stream>>>(e->st.keys, n, len_k, out);
+}
+using LongBitsFn = void (*)(mpx_engine *, uint64_t, uint32_t, uint32_t *, unsigned);
+LongBitsFn pick_long_bits(int W) {
+    switch (W) {
+    case 1: return &launch_long_bits<1>;
+    case 2: return &launch_long_bits<2>;
+    case 3: return &launch_long_bits<3>;
+    case 4: return &launch_long_bits<4>;
+    case 5: return &launch_long_bits<5>;
+    case 6: return &launch_long_bits<6>;
+    case 7: return &launch_long_bits<7>;
+    default: return &launch_long_bits<8>;
     }
 }
 
@@ -1082,6 +1113,7 @@ void free_adjoint(mpx_engine *e) {
     dev_free(e, e->adj.r_tgt);
     dev_free(e, e->adj.r_code);
     dev_free(e, e->adj.r_begin);
+    dev_free(e, e->adj.longb);
     e->adj = AdjointState{};
     e->fwd_tape = Tape{};
 }
@@ -1144,6 +1176,17 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
         e->rec_hint = std::max(e->rec_hint, e->adj.r_total);
     }
     e->fwd_tape = Tape{};
+    if (e->tr.has_len_k) {
+        // only_rotate_len_k: which terms of the final store lie outside every gate's rotation set
+        e->adj.len_k = e->tr.len_k;
+        const uint64_t words = std::max<uint64_t>((n + 31) / 32, 1);
+        MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.longb), words * sizeof(uint32_t)));
+        if (n > 0) {
+            const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 4096));
+            pick_long_bits(e->W)(e, n, e->tr.len_k, e->adj.longb, blocks);
+            ++e->launches;
+        }
+    }
     MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&e->adj.final_coef), std::max<uint64_t>(n, 1) * sizeof(double)));
     if (n > 0)
         MPX_CUDA(cudaMemcpyAsync(e->adj.final_coef, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
@@ -1332,6 +1375,7 @@ mpx_status recorded_view(mpx_engine *eng, FrozenGraph &v) {
     v.code = A.r_code;
     v.p_begin = A.r_begin;
     v.w_anti = A.w_anti;
+    v.longb = A.longb;
     v.n0.resize(L);
     v.anti.resize(L);
     v.count.resize(L);
@@ -1350,7 +1394,7 @@ void free_graph(mpx_engine *e) {
     FrozenGraph &g = e->fg;
     for (void *p : {static_cast<void *>(g.src), static_cast<void *>(g.tgt), static_cast<void *>(g.code),
                     static_cast<void *>(g.p_begin), static_cast<void *>(g.p_count), static_cast<void *>(g.w_anti),
-                    static_cast<void *>(g.done), static_cast<void *>(g.last)})
+                    static_cast<void *>(g.done), static_cast<void *>(g.last), static_cast<void *>(g.longb)})
         dev_free(e, p);
     g = FrozenGraph{};
 }
@@ -1393,7 +1437,7 @@ mpx_status graph_pare(mpx_engine *eng, double threshold) {
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&g.last), std::max<uint64_t>(g.n_final, 1) * sizeof(int32_t)));
     // |weight| = 1 on fully paired terms: kept iff 1 > threshold
     pick_pare_init(e->W)(e, g.n_final, 1.0 > threshold ? 1 : 0, static_cast<int32_t>(g.L) - 1, g.last);
-    const Frozen fz = Frozen{g.src, g.tgt, g.code, g.p_begin, g.p_count, nullptr};
+    const Frozen fz = Frozen{g.src, g.tgt, g.code, g.p_begin, g.p_count, nullptr, nullptr};
     for (uint64_t st = g.L; st-- > 0;) {
         const uint64_t cnt = g.count[st];
         if (cnt == 0) continue;
@@ -1442,6 +1486,7 @@ mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_g
         A.r_tgt = nullptr;
         A.r_code = nullptr;
         A.r_begin = nullptr;
+        A.longb = nullptr; // owned by the graph now
         A.w_anti = nullptr;
         free_adjoint(e);
         MPX_CUDA(cudaStreamSynchronize(e->stream));
@@ -1553,7 +1598,9 @@ mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_g
         g.n0[st] = A.stats[4 * st];
         g.anti[st] = A.stats[4 * st + 1];
     }
-    g.w_anti = A.w_anti; // the graph keeps the per-warp counts
+    g.w_anti = A.w_anti; // the graph keeps the per-warp counts and the outside-set bits
+    g.longb = A.longb;
+    A.longb = nullptr;
     A.w_anti = nullptr;
     free_adjoint(e);
     MPX_CUDA(cudaStreamSynchronize(e->stream));
@@ -2114,8 +2161,6 @@ mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t seg
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
-    if (e->tr.has_len_k)
-        return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
     if (e->schr)
         return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
                                         "the gradient or graph)");
@@ -2134,7 +2179,15 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
                                         "with no propagation in between");
     MPX_CUDA(cudaSetDevice(e->device));
     if (c->n == 0) return MPX_OK;
-    if (!e->adj.rec_ok) return adjoint_backward(e, *c, grad_angles);
+    if (!e->adj.rec_ok) {
+        // the streaming replay runs with the forward pass's only_rotate_len_k
+        const Trunc saved = e->tr;
+        e->tr.has_len_k = e->adj.len_k > 0;
+        e->tr.len_k = e->adj.len_k;
+        const mpx_status s = adjoint_backward(e, *c, grad_angles);
+        e->tr = saved;
+        return s;
+    }
     // The forward pass recorded every gate's pairs: replay the segments with the frozen kernels.
     FrozenGraph view;
     mpx_status s = recorded_view(e, view);
@@ -2148,8 +2201,6 @@ mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
-    if (e->tr.has_len_k)
-        return fail(eng, MPX_ERR_INVALID, "only_rotate_len_k is supported by propagate only (not by the gradient or graph)");
     if (e->schr)
         return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
                                         "the gradient or graph)");

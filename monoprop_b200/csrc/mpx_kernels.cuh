@@ -253,6 +253,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
 #pragma unroll
                         for (int w = 0; w < W; ++w) kp += __popcll(mk[w]);
                         member = kp <= static_cast<int>(tr.len_k);
+                        if constexpr (REPLAY) {
+                            // its undo slot says "not scaled by this gate" (the backward pass skips it)
+                            if (!member) {
+                                const uint64_t rr = s_ubase[ow] + static_cast<uint64_t>(k + kBlock * r +
+                                                                                         static_cast<int>(threadIdx.x) -
+                                                                                         static_cast<int>(s_wpfx[ow]));
+                                tp.u_idx[rr] = kNoStall;
+                            }
+                        }
                     }
                     if (member) {
                         follower = (s_foll[ow][word] >> (l & 31)) & 1u;
@@ -338,13 +347,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Count
 // term's pre-gate value goes to the undo log from its chunk-owning warp's offset (pair members' entries
 // are never read).
 // With a pared graph (last != nullptr) a term whose value can no longer reach <0|O|0> after this step
-// (last[term] < step) keeps its coefficient unscaled.
+// (last[term] < step) keeps its coefficient unscaled. With a graph built under only_rotate_len_k, longb
+// (one bit per term) marks the terms of more than k slots: they are never scaled, and their undo entries
+// say so (index kNoStall).
 template <int W, bool LOG>
 __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
     k_frozen_scan(Store st, const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step, uint64_t n0,
-                  uint32_t *__restrict__ done, Tape tp, const int32_t *__restrict__ last) {
+                  uint32_t *__restrict__ done, Tape tp, const int32_t *__restrict__ last,
+                  const uint32_t *__restrict__ longb) {
     __shared__ uint32_t s_anti[kWarps][kBatch * 32];
     __shared__ uint32_t s_done[kWarps][kBatch * 32];
+    __shared__ uint32_t s_long[kWarps][kBatch * 32];
     __shared__ uint32_t s_pfx[kWarps][kBatch * 32];
     __shared__ uint32_t s_wtot[kWarps];
     __shared__ uint32_t s_wpfx[kWarps + 1];
@@ -380,7 +393,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
 #pragma unroll 2
         for (int b = 0; b < nb; ++b) {
             const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
-            uint32_t anti = 0, dn = 0;
+            uint32_t anti = 0, dn = 0, lg = 0; // lg: terms outside the only_rotate_len_k set
             if (j < geo.nwords) {
                 if (n_fold <= kMaxFoldCols) {
                     uint32_t v[kMaxFoldCols];
@@ -403,6 +416,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                 if (j == geo.nwords - 1) anti &= tail;
                 dn = done[j];
                 if (dn) done[j] = 0;
+                if (longb != nullptr) lg = longb[j];
             }
             const int cnt_l = __popc(anti);
             int incl = cnt_l;
@@ -413,6 +427,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
             }
             s_anti[warp][b * 32 + lane] = anti;
             s_done[warp][b * 32 + lane] = dn;
+            s_long[warp][b * 32 + lane] = lg;
             s_pfx[warp][b * 32 + lane] = static_cast<uint32_t>(total + incl - cnt_l);
             total += __shfl_sync(0xFFFFFFFFu, incl, 31);
         }
@@ -436,7 +451,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
             uint64_t term[kPrefetch];
             double vv[kPrefetch];
             int own[kPrefetch];
-            bool skip[kPrefetch];
+            bool skip[kPrefetch], outside[kPrefetch];
 #pragma unroll
             for (int r = 0; r < kPrefetch; ++r) {
                 const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
@@ -444,6 +459,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                 term[r] = 0;
                 vv[r] = 0.0;
                 skip[r] = true;
+                outside[r] = false;
                 if (idx < btotal) {
                     int ow = 0;
 #pragma unroll
@@ -460,7 +476,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                                            static_cast<uint64_t>(lo >> 5) * geo.n_warps;
                     own[r] = ow;
                     term[r] = chunk * 1024 + static_cast<uint64_t>(lo & 31) * 32 + bit;
-                    skip[r] = (s_done[ow][lo] >> bit) & 1u;
+                    outside[r] = (s_long[ow][lo] >> bit) & 1u;
+                    skip[r] = ((s_done[ow][lo] >> bit) & 1u) || outside[r];
                     vv[r] = st.coef[term[r]];
                 }
             }
@@ -470,7 +487,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                 if constexpr (LOG) {
                     const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
                     const uint64_t rr = s_ubase[own[r]] + static_cast<uint64_t>(idx - static_cast<int>(s_wpfx[own[r]]));
-                    tp.u_idx[rr] = static_cast<uint32_t>(term[r]);
+                    tp.u_idx[rr] = outside[r] ? kNoStall : static_cast<uint32_t>(term[r]);
                     tp.u_val[rr] = vv[r];
                 }
                 if (!skip[r] && (last == nullptr || last[term[r]] >= static_cast<int32_t>(step)))
@@ -642,6 +659,9 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     rec = true; // a rotated pair (recorded in replay mode and by a recording forward pass)
                     tgt = static_cast<uint32_t>(found);
                     code = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
+                    // 0x20: the partner lies outside the only_rotate_len_k set (no cos factor of its own)
+                    if constexpr (LENK)
+                        if (fpop > static_cast<int>(tr.len_k)) code = static_cast<int8_t>(code | 0x20);
                 }
             }
         }
@@ -733,7 +753,7 @@ __global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counte
                     if (r < tp.r_cap) {
                         tp.r_src[r] = src;
                         tp.r_tgt[r] = miss ? static_cast<uint32_t>(s_base + off + __popc(ball & lt_mask)) : tgt;
-                        tp.r_code[r] = static_cast<int8_t>((miss ? 0x10 : 0) | (static_cast<int>(ph) & 0xF));
+                        tp.r_code[r] = miss ? static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF)) : code;
                     }
                 }
             }
@@ -891,6 +911,28 @@ __global__ void __launch_bounds__(kBlock) k_expect_schr(const uint32_t *__restri
     }
     const double total = block_sum(acc, s_red);
     if (threadIdx.x == 0) out[0] = core + total;
+}
+
+// One bit per term (column-word layout): set when the term has more than len_k set slots, i.e. lies
+// outside the only_rotate_len_k set of every gate (Scan.h:146-157).
+template <int W>
+__global__ void k_long_bits(const uint64_t *__restrict__ keys, uint64_t n, uint32_t len_k, uint32_t *__restrict__ out) {
+    const uint64_t words = (n + 31) >> 5;
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) & ~uint64_t(31);
+         base < words * 32; base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i = base + (threadIdx.x & 31);
+        bool is_long = false;
+        if (i < n) {
+            uint64_t m[W];
+            load_key<W>(keys, i, m);
+            int pop = 0;
+#pragma unroll
+            for (int w = 0; w < W; ++w) pop += __popcll(m[w]);
+            is_long = pop > static_cast<int>(len_k);
+        }
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, is_long);
+        if ((threadIdx.x & 31) == 0) out[base >> 5] = b;
+    }
 }
 
 // coef[idx[k]] = val[k] (indices distinct).

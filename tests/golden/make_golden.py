@@ -138,6 +138,39 @@ def full_depth() -> None:
         print("full", name, wl.n_layers, r.keys.shape[0], r.expectation, f"{r.seconds:.1f} s", flush=True)
 
 
+#: frozen graphs built with only_rotate_len_k: (name, workload, layers, k)
+GRAPHS_LEN_K = [("hubbard6x6_L300_k4", W.hubbard6x6, 300, 4), ("ising100_L600_k6", W.ising100, 600, 6)]
+
+
+def graphs_len_k() -> None:
+    """graph_<name>.npz for graphs built with only_rotate_len_k (build_graph's argument, binder.h:102-110):
+    the reference's replay at the build parameters and at shifted ones (seed 77, 0.05 N(0, 1)) with its
+    gradient there, plus central finite differences (h = 1e-5) of the replay on 32 seeded parameters."""
+    for name, make, L, k in GRAPHS_LEN_K:
+        wl = make()
+        wl = dataclasses.replace(wl, extra={**wl.extra, "only_rotate_len_k": k})
+        eng = oracle.RefEngine(wl)
+        eng.propagate(n_layers=L, build_graph=True)
+        n_params = int(wl.param_map[:L].max()) + 1
+        theta = wl.params[:n_params]
+        shifted = theta + 0.05 * np.random.default_rng(77).standard_normal(n_params)
+        ev, grad, _ = eng.expectation_and_gradient(shifted)
+        ev0 = eng.expectation(theta)
+        idx = np.sort(np.random.default_rng(5).choice(n_params, size=min(32, n_params), replace=False))
+        h = 1e-5
+        fd = np.zeros(idx.size)
+        for j, p in enumerate(idx):
+            tp, tm = shifted.copy(), shifted.copy()
+            tp[p] += h
+            tm[p] -= h
+            fd[j] = (eng.expectation(tp) - eng.expectation(tm)) / (2 * h)
+        eng.close()
+        np.savez_compressed(os.path.join(HERE, f"graph_{name}.npz"), expectation=np.float64(ev),
+                            expectation_build=np.float64(ev0), grad=grad, params=shifted, n_layers=np.int64(L),
+                            only_rotate_len_k=np.int64(k), fd_idx=idx, fd=fd)
+        print("graph len_k", name, ev0, ev, float(np.abs(grad).max()), float(np.max(np.abs(grad[idx] - fd))))
+
+
 def surface(reference_root: str) -> None:
     """The names the reference's nanobind module binds per propagator class and module-wide
     (``src/monoprop/bindings/binder.h``, ``bindings.cpp.in``), and the ``_simulator`` attributes its Python
@@ -176,6 +209,9 @@ def main(reference_root: str | None = None) -> None:
         return
     if "--surface" in sys.argv:
         surface(reference_root)
+        return
+    if "--graph-len-k" in sys.argv:
+        graphs_len_k()
         return
     for name, make, L, k in LEN_K:
         wl = make()

@@ -3,7 +3,8 @@
 The reference (Scan.h:146-157,376-391, FusedApply.h:46-52) skips them in the cos set and in the emit
 pass, and a partner outside the set receives its sine term unscaled. Checked against the golden fixtures
 generated by the reference with only_rotate_len_k, against the oracle on seeded random circuits (Pauli
-and Majorana), and through the _core module (validation message, gradient/graph rejection).
+and Majorana), and through the _core module (validation message); graphs and gradients built with only_rotate_len_k
+against the reference's own graph and its finite differences.
 """
 
 import dataclasses
@@ -60,10 +61,6 @@ def test_len_k_cleared_and_guards():
     circ = eng.upload(wl.gen_words(), wl.angles())
     eng.set_only_rotate_len_k(6)
     with pytest.raises(_native.MpxInvalid):
-        eng.adjoint_forward(circ)
-    with pytest.raises(_native.MpxInvalid):
-        eng.graph_build(circ)
-    with pytest.raises(_native.MpxInvalid):
         eng.set_only_rotate_len_k(2 * wl.num_modes + 1)
     eng.set_only_rotate_len_k(None)  # cleared: a plain propagation again
     eng.propagate_circuit(circ)
@@ -89,3 +86,87 @@ def test_core_propagate_only_rotate_len_k():
     assert p.size() == int(g["n"])
     assert abs(p.expectation_value([]) - float(g["expectation"])) <= 1e-10
     assert _core.MAX_NUM_MODES >= wl.num_modes
+
+
+LEN_K_GRAPHS = {"hubbard6x6_L300_k4": ("hubbard6x6", 300, 4), "ising100_L600_k6": ("ising100", 600, 6)}
+
+
+def _core_graph(name):
+    """A _core propagator (the reference's class layout) holding the graph of LEN_K_GRAPHS[name], built with
+    only_rotate_len_k at the workload's parameters."""
+    from monoprop_b200 import workloads as W
+    from monoprop_b200.propagators import dispatch
+
+    base, L, k = LEN_K_GRAPHS[name]
+    wl = W.BY_NAME[base]()
+    ops = {tuple(key): complex(v) for key, v in wl.observable.items()}
+    p = dispatch(wl.num_modes)(initial_operator=ops, cutoff=wl.cutoff, initial_state=list(wl.initial_state),
+                               cutoff_type=wl.cutoff_type, lower_atol=wl.lower_atol, logical_num_modes=wl.num_modes,
+                               basis=wl.basis)
+    P = int(wl.param_map[:L].max()) + 1
+    p.build_graph([list(m) for m in wl.gate_slots[:L]], list(map(int, wl.param_map[:L])), list(wl.gen_coeffs[:L]),
+                  None, list(wl.params[:P]), k)
+    return wl, L, k, P, p
+
+
+@pytest.mark.parametrize("name", sorted(LEN_K_GRAPHS))
+def test_len_k_graph_matches_reference(name):
+    """build_graph(..., only_rotate_len_k=k) (binder.h:102-110): the replay at the build parameters, and
+    <O> and the gradient at shifted parameters, against the reference's own graph (tests/golden/graph_*_k*.npz),
+    plus per-angle central finite differences of the reference's replay (1e-7 relative + 1e-9)."""
+    g = golden.load("graph_" + name)
+    wl, L, k, P, p = _core_graph(name)
+    ev0 = p.expectation_value(list(wl.params[:P]))
+    assert abs(ev0 - float(g["expectation_build"])) <= 1e-10 * max(1.0, abs(float(g["expectation_build"])))
+    ev, grad = p.expectation_value_and_gradient(list(g["params"]))
+    grad = np.asarray(grad)
+    assert abs(ev - float(g["expectation"])) <= 1e-10 * max(1.0, abs(float(g["expectation"])))
+    assert np.max(np.abs(grad - g["grad"])) <= 1e-9 * max(1.0, np.max(np.abs(g["grad"])))
+    fd = g["fd"]
+    assert np.all(np.abs(grad[g["fd_idx"]] - fd) <= 1e-7 * np.abs(fd) + 1e-9)
+
+
+def test_len_k_graph_replay_is_the_propagation():
+    """At its build parameters the replayed graph is the only_rotate_len_k propagation itself: the same
+    coefficients as the reference's propagate (tests/golden/hubbard6x6_L400_k4.npz)."""
+    from monoprop_b200 import workloads as W
+    from monoprop_b200.propagators import dispatch
+
+    wl = W.hubbard6x6()
+    L, k = 400, 4
+    ops = {tuple(key): complex(v) for key, v in wl.observable.items()}
+    p = dispatch(wl.num_modes)(initial_operator=ops, cutoff=wl.cutoff, initial_state=list(wl.initial_state),
+                               cutoff_type="length", lower_atol=wl.lower_atol, logical_num_modes=wl.num_modes)
+    P = int(wl.param_map[:L].max()) + 1
+    p.build_graph([list(m) for m in wl.gate_slots[:L]], list(map(int, wl.param_map[:L])), list(wl.gen_coeffs[:L]),
+                  None, list(wl.params[:P]), k)
+    ev = p.expectation_value(list(wl.params[:P]))
+    g = golden.load("hubbard6x6_L400_k4")
+    assert p.size() == int(g["n"]) and abs(ev - float(g["expectation"])) <= 1e-10
+    coefs = np.asarray(p.contract_partially(list(wl.params[:P]), False))
+    assert np.allclose(np.sort(coefs), np.sort(g["coefs"]), rtol=1e-10, atol=1e-15)
+
+
+@pytest.mark.parametrize("pair_log", [-1, 0])
+def test_len_k_adjoint_equals_graph_gradient(pair_log):
+    """The engine's adjoint with only_rotate_len_k (forward pair log replayed by the frozen kernels, or,
+    without the log, the streaming kernels in replay mode) gives the graph's gradient at the same angles."""
+    from monoprop_b200 import workloads as W
+
+    wl = W.hubbard6x6()
+    L, k = 300, 4
+    eng = _native.engine_for(wl)
+    eng.set_pair_log(pair_log)
+    circ = eng.upload(wl.gen_words()[:L], wl.angles()[:L])
+    eng.set_only_rotate_len_k(k)
+    ev = eng.adjoint_forward(circ, 64)
+    eng.set_only_rotate_len_k(None)  # the backward pass keeps the forward pass's k
+    ga = eng.adjoint_backward(circ)
+    eng.set_only_rotate_len_k(k)
+    eng.graph_build(circ)
+    eng.set_only_rotate_len_k(None)
+    ev_g, gg = eng.graph_gradient(circ)
+    circ.close()
+    eng.close()
+    assert abs(ev - ev_g) <= 1e-13 * max(1.0, abs(ev))
+    assert np.max(np.abs(ga - gg)) <= 1e-11 * max(1.0, np.max(np.abs(gg)))
