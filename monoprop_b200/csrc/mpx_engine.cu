@@ -1972,7 +1972,7 @@ mpx_status mpx_expectation(mpx_engine *e, double *out) {
     }
     else {
         pick_exp(e->W, e->cfg.basis)(e);
-        k_expect_final<<<1, 32, 0, e->stream>>>(e->d_partial, static_cast<uint32_t>(e->grid), e->core, e->d_out);
+        k_expect_final<<<1, kBlock, 0, e->stream>>>(e->d_partial, static_cast<uint32_t>(e->grid), e->core, e->d_out);
         e->launches += 2;
     }
     MPX_CUDA(cudaGetLastError());

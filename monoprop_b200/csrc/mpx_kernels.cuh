@@ -39,8 +39,16 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 
 constexpr int kWarps = kBlock / 32;
 constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
-constexpr int kPrefetch = 4;         // anticommuting terms per lane whose coefficient loads are in flight together
-constexpr int kBatch = 8;            // chunks per warp whose column scans are issued together
+// Build-time tuning of the sweep (nvcc -D...): anticommuting terms per lane whose coefficient loads are in
+// flight together, and chunks per warp whose column scans are issued together.
+#ifndef MPX_SWEEP_PREFETCH
+#define MPX_SWEEP_PREFETCH 4
+#endif
+#ifndef MPX_SWEEP_BATCH
+#define MPX_SWEEP_BATCH 8
+#endif
+constexpr int kPrefetch = MPX_SWEEP_PREFETCH;
+constexpr int kBatch = MPX_SWEEP_BATCH;
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
 // warp w of block b scans the 1024-term chunks b + grid * (w + warps * i); block b owns the query
@@ -982,13 +990,14 @@ __global__ void __launch_bounds__(kBlock) k_expect(Store st, const Counters *__r
     }
 }
 
-__global__ void k_expect_final(const double *__restrict__ partial, uint32_t nblocks, double core,
-                               double *__restrict__ out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double t = 0.0;
-        for (uint32_t b = 0; b < nblocks; ++b) t += partial[b];
-        out[0] = core + t;
-    }
+// core + the block partials, one block: every thread sums a fixed strided subset, then a fixed-order tree.
+__global__ void __launch_bounds__(kBlock) k_expect_final(const double *__restrict__ partial, uint32_t nblocks,
+                                                          double core, double *__restrict__ out) {
+    __shared__ double s_red[kBlock / 32];
+    double t = 0.0;
+    for (uint32_t b = threadIdx.x; b < nblocks; b += kBlock) t += partial[b];
+    const double total = block_sum(t, s_red);
+    if (threadIdx.x == 0) out[0] = core + total;
 }
 
 } // namespace mpx
