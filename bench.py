@@ -410,8 +410,8 @@ def main() -> None:
                 "anticommuting_per_step": int(anti.sum()), "emitted_per_step": int(emitted.sum()),
                 "appended_per_step": int(app.sum()),
                 "path_frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak}
-    # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on the
-    # 8 M-term profiling case, see profiles/) scaled to this workload's algorithmic bytes per launch.
+    # DRAM bytes per launch: the ncu-measured traffic/algorithmic ratio of the sweep (captured on this
+    # circuit itself at 8.0e6 terms, `--regime-case`), scaled to the average launch's algorithmic bytes.
     traffic_file = os.path.join(ROOT, "profiles", "k_sweep_traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
