@@ -177,8 +177,10 @@ MPX_API mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, dou
 /* Batch of independent problems (observable + circuit + angles each) on one GPU. No reference
  * counterpart: the reference runs one propagator per process (its benches loop over instances). Items
  * are spread over opt->workers host threads, each with its own engine and CUDA stream, deepest circuit
- * first, so the per-gate kernels of different instances share the GPU; an instance that runs out of device
- * memory waits for another to finish and retries. Per item: <0|O|0> into *expectation, and with
+ * first, so the per-gate kernels of different instances share the GPU. An instance starts only while the
+ * expected device footprints of the running ones (learned from the finished instances at least as deep)
+ * fit the free memory measured at the start; one that still runs out of device memory waits for another
+ * to finish and retries. Per item: <0|O|0> into *expectation, and with
  * opt->gradient d<0|O|0>/d(angle_l) into grad_angles[n_layers] (when non-NULL). */
 typedef struct {
     const uint64_t *obs_words; /* [n_obs][W] */

@@ -5,8 +5,11 @@
 // each driving its own engine and CUDA stream, so the per-gate kernels of different instances run
 // concurrently on the GPU: small or shallow instances, which cannot fill 148 SMs alone, share the
 // machine, and the deepest instances start first (longest-processing-time order) so the tail is short.
-// Device memory is bounded by admission: an instance that fails to allocate waits until another worker
-// finishes and retries; only an instance that cannot fit on an otherwise idle GPU is an error.
+// Device memory is bounded by planned admission: an instance starts only while the expected footprints of
+// the running instances fit the free memory measured at the start (expectations learned from the
+// instances already finished, see Admission); an allocation failure that still happens waits until
+// another worker finishes and retries; only an instance that cannot fit on an otherwise idle GPU is an
+// error.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +32,29 @@ extern "C" mpx_status mpx_internal_create_shared(const mpx_config *cfg, const ui
 
 namespace {
 
+// Memory admission. Instances start only while the device memory the running ones are expected to need
+// fits a budget (the free memory when the batch starts, less a margin). An instance's expectation comes
+// from the instances already finished: the largest measured footprint among those at least as deep
+// (instances run deepest first, so this is an upper bound by depth), or, before any has finished, an equal
+// share of the budget per worker. An allocation failure still waits for a release and retries.
+struct Admission {
+    uint64_t budget = 0;                          // bytes; 0 = no planning (free memory unknown)
+    uint64_t reserved = 0;                        // expected bytes of the running instances
+    std::vector<std::pair<uint64_t, uint64_t>> seen; // (layers, measured bytes) of finished instances
+    uint64_t fair_share = 0;
+
+    uint64_t expect(uint64_t layers) const {
+        uint64_t best = 0;
+        bool any = false;
+        for (const auto &[l, b] : seen)
+            if (l >= layers) {
+                best = std::max(best, b);
+                any = true;
+            }
+        return any ? best : fair_share;
+    }
+};
+
 struct BatchState {
     std::mutex mu;
     std::condition_variable cv;
@@ -38,10 +64,23 @@ struct BatchState {
     std::atomic<bool> failed{false};
     mpx_status status = MPX_OK;
     std::string error;
+    Admission adm;
 };
 
-// One instance on a fresh engine (the device memory pool makes engine creation cheap).
-mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_options &opt, std::string &err) {
+// Device bytes an engine holds at the end of its instance (store, table, columns, scratch, graph), with
+// the gradient's checkpoints and tape on top when it ran one.
+uint64_t footprint(mpx_engine *e, bool gradient) {
+    mpx_memory_info m{};
+    if (mpx_memory(e, &m) != MPX_OK) return 0;
+    const uint64_t b = m.key_bytes + m.coef_bytes + m.table_bytes + m.column_bytes + m.scratch_bytes + m.initial_bytes +
+                       m.graph_bytes;
+    return gradient ? 2 * b : b + b / 4;
+}
+
+// One instance on a fresh engine (the device memory pool makes engine creation cheap). *bytes: its
+// measured footprint.
+mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_options &opt, std::string &err,
+                   uint64_t *bytes) {
     mpx_engine *e = nullptr;
     mpx_status s = mpx_internal_create_shared(&cfg, it.obs_words, it.obs_coef, it.n_obs, it.core, it.state_mask, &e);
     if (s != MPX_OK) {
@@ -64,6 +103,7 @@ mpx_status run_one(const mpx_config &cfg, mpx_batch_item &it, const mpx_batch_op
             s = mpx_export(e, it.export_words, it.export_coefs, it.export_cap, it.export_n);
     }
     if (s != MPX_OK) err = mpx_last_error(e);
+    if (s == MPX_OK && bytes != nullptr) *bytes = footprint(e, opt.gradient && it.grad_angles != nullptr);
     mpx_circuit_destroy(c);
     mpx_destroy(e);
     return s;
@@ -87,19 +127,30 @@ void worker(const mpx_config &cfg, mpx_batch_item *items, const std::vector<uint
         if (k >= order.size()) return;
         mpx_batch_item &it = items[order[k]];
         for (;;) {
-            uint64_t seen;
+            uint64_t seen, want;
             {
-                std::lock_guard<std::mutex> lock(bs.mu);
+                // admission: wait until the expected footprint fits the budget (or nothing else runs)
+                std::unique_lock<std::mutex> lock(bs.mu);
+                want = bs.adm.expect(it.n_layers);
+                bs.cv.wait(lock, [&] {
+                    return bs.adm.budget == 0 || bs.in_flight == 0 || bs.adm.reserved + want <= bs.adm.budget ||
+                           bs.failed.load();
+                });
+                if (bs.failed.load()) return;
+                bs.adm.reserved += want;
                 ++bs.in_flight;
                 seen = bs.completions;
             }
             std::string err;
-            const mpx_status s = run_one(cfg, it, opt, err);
+            uint64_t bytes = 0;
+            const mpx_status s = run_one(cfg, it, opt, err, &bytes);
             int others;
             {
                 std::lock_guard<std::mutex> lock(bs.mu);
                 --bs.in_flight;
                 ++bs.completions;
+                bs.adm.reserved -= want;
+                if (s == MPX_OK && bytes > 0) bs.adm.seen.emplace_back(it.n_layers, bytes);
                 others = bs.in_flight;
             }
             bs.cv.notify_all();
@@ -158,6 +209,18 @@ MPX_API mpx_status mpx_batch_run(const mpx_config *cfg, mpx_batch_item *items, u
     const int workers = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(opt->workers > 0 ? opt->workers : 8,
                                                                                  std::max<uint64_t>(n_items, 1))));
     BatchState bs;
+    {
+        // the admission budget: the device's free memory now, less a 10 % margin
+        int prev = 0;
+        cudaGetDevice(&prev);
+        size_t free_b = 0, total_b = 0;
+        if (cudaSetDevice(cfg->device) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            bs.adm.budget = free_b - free_b / 10;
+            bs.adm.fair_share = bs.adm.budget / static_cast<uint64_t>(workers);
+        }
+        cudaGetLastError();
+        cudaSetDevice(prev);
+    }
     std::vector<std::thread> pool;
     pool.reserve(workers);
     for (int w = 0; w < workers; ++w) pool.emplace_back(worker, std::cref(*cfg), items, std::cref(order), std::cref(*opt),

@@ -38,7 +38,11 @@ __device__ __forceinline__ int nth_set_bit(uint32_t a, int r) {
 }
 
 constexpr int kWarps = kBlock / 32;
-constexpr int kSweepBlocksPerSM = 4; // the sweep's register budget (64 / thread) fits 4 blocks per SM
+// Resident blocks per SM the per-gate kernels are compiled for (register budget 65536 / (256 x this)).
+#ifndef MPX_SWEEP_BLOCKS
+#define MPX_SWEEP_BLOCKS 4
+#endif
+constexpr int kSweepBlocksPerSM = MPX_SWEEP_BLOCKS;
 // Build-time tuning of the sweep (nvcc -D...): anticommuting terms per lane whose coefficient loads are in
 // flight together, and chunks per warp whose column scans are issued together.
 #ifndef MPX_SWEEP_PREFETCH
@@ -81,7 +85,7 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 // index and pre-gate coefficient go to the undo log at its chunk-owning warp's precomputed offset.
 // EXT: bit 0 only_rotate_len_k, bit 1 basis_change (instantiated only where the engine uses them).
 template <int W, int BASIS, bool REPLAY = false, int EXT = 0>
-__global__ void __launch_bounds__(kBlock, 4) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
+__global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                    const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                    Trunc tr, Tape tp, uint64_t *__restrict__ stats) {
     __shared__ uint32_t s_anti[kWarps][kBatch * 32];
@@ -523,7 +527,7 @@ constexpr int kMaxGrid = 1024; // largest per-gate grid (148 SMs x at most 4 blo
 // append it was, nothing is inserted, and every rotated or appended pair goes to the tape's pair log with
 // both pre-gate coefficients (one counter bump per round).
 template <int W, int BASIS, bool REPLAY = false, bool LENK = false>
-__global__ void __launch_bounds__(kBlock) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
+__global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st, Scratch sc, Counters *__restrict__ cnt,
                                                      const GateDesc *__restrict__ gates, uint32_t gate, uint32_t step,
                                                      Trunc tr, Tape tp) {
     __shared__ uint32_t warp_cnt[kWarps];
