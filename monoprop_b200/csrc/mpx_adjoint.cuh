@@ -240,6 +240,73 @@ __global__ void __launch_bounds__(kBlock) k_adj_undo(Tape tp, const GateDesc *__
     }
 }
 
+// One reverse step as a single launch, for segments replayed with the frozen kernels: their undo log marks
+// pair members with the skip index, so the pair records and the undo entries touch disjoint adjoint
+// entries and need no done bits. The step's work is the pair records followed by the undo entries, dealt
+// grid-stride over all blocks; each block's share of dE/dangle goes to its slot, and the last block to
+// finish writes grad[gate] as the fixed-order sum of the slots (the same arithmetic per record as
+// k_adj_pairs and k_adj_undo).
+__global__ void __launch_bounds__(kBlock) k_adj_step(Tape tp, const GateDesc *__restrict__ gates, uint32_t gate,
+                                                      uint32_t step, double *__restrict__ lam, GradPartials gp,
+                                                      double *__restrict__ grad) {
+    __shared__ double s_red[kBlock / 32];
+    __shared__ bool s_last;
+    pdl_trigger();
+    pdl_wait();
+    const uint64_t pbase = tp.p_base[step], pcnt = tp.p_cnt[step];
+    const uint64_t ubase = tp.u_base[step], ucnt = tp.u_cnt[step];
+    const uint64_t total = pcnt + ucnt;
+    const GateDesc &gd = gates[gate];
+    const double C = gd.cosv, S = gd.sinv;
+    double acc = 0.0;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(kBlock) + threadIdx.x; k < total;
+         k += static_cast<uint64_t>(gridDim.x) * kBlock) {
+        if (k < pcnt) {
+            const uint64_t r = pbase + k;
+            const uint32_t s = tp.p_src[r], t = tp.p_tgt[r];
+            const int8_t code = tp.p_code[r];
+            const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
+            const double vs = tp.p_vs[r], vt = tp.p_vt[r];
+            const double ls = lam[s], lt = lam[t];
+            if (code & 0x20) { // partner outside the only_rotate_len_k set: c_T' = c_T + s phi c_S
+                acc += ls * (-2.0 * S * vs - 2.0 * C * phi * vt) + lt * (2.0 * C * phi * vs);
+                lam[s] = C * ls + S * phi * lt;
+                lam[t] = lt - S * phi * ls;
+            }
+            else {
+                acc += ls * (-2.0 * S * vs - 2.0 * C * phi * vt) + lt * (-2.0 * S * vt + 2.0 * C * phi * vs);
+                lam[s] = C * ls + S * phi * lt;
+                if ((code & 0x10) == 0) lam[t] = C * lt - S * phi * ls;
+            }
+        }
+        else {
+            const uint64_t r = ubase + (k - pcnt);
+            const uint32_t i = tp.u_idx[r];
+            if (i != kNoStall) {
+                const double l = lam[i];
+                acc += l * (-2.0 * S * tp.u_val[r]);
+                lam[i] = C * l;
+            }
+        }
+    }
+    const double t = block_sum(acc, s_red);
+    if (threadIdx.x == 0) {
+        gp.part[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(gp.arrivals, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double v = 0.0;
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) v += __ldcg(gp.part + k);
+    const double sum = block_sum(v, s_red);
+    if (threadIdx.x == 0) {
+        grad[gate] = sum;
+        *gp.arrivals = 0u;
+    }
+}
+
 }  // namespace mpx
 
 namespace mpx {

@@ -1326,12 +1326,19 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         }
         for (uint64_t st = hi; st-- > lo;) {
             const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
-            launch_dep(e, &k_adj_pairs, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
-                       done, gp);
-            launch_dep(e, &k_adj_undo, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
-                       done, gp, grad);
+            if (fg != nullptr) {
+                // frozen replay: pair members carry the skip index in the undo log, one launch per step
+                launch_dep(e, &k_adj_step, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st),
+                           lam, gp, grad);
+            }
+            else {
+                launch_dep(e, &k_adj_pairs, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st),
+                           lam, done, gp);
+                launch_dep(e, &k_adj_undo, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st),
+                           lam, done, gp, grad);
+            }
         }
-        e->launches += 5 * (hi - lo) + 1;
+        e->launches += (fg != nullptr ? 3 : 5) * (hi - lo) + 1;
         MPX_CUDA_REL(cudaGetLastError());
     }
     e->launches += 1;

@@ -356,8 +356,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
 // scaled by cos; pair members (done bits, set by k_frozen_pairs) are skipped and their bits cleared.
 // Chunk ownership, batching and the block-wide dealing of the anticommuting terms are the sweep's, so
 // each sweep warp's terms are the ones it counted in the forward pass. With LOG every anticommuting
-// term's pre-gate value goes to the undo log from its chunk-owning warp's offset (pair members' entries
-// are never read).
+// term's pre-gate value goes to the undo log from its chunk-owning warp's offset; pair members get the
+// skip index kNoStall there (their adjoint comes from the pair records: k_adj_step).
 // With a pared graph (last != nullptr) a term whose value can no longer reach <0|O|0> after this step
 // (last[term] < step) keeps its coefficient unscaled. With a graph built under only_rotate_len_k, longb
 // (one bit per term) marks the terms of more than k slots: they are never scaled, and their undo entries
@@ -499,7 +499,9 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                 if constexpr (LOG) {
                     const int idx = k + kBlock * r + static_cast<int>(threadIdx.x);
                     const uint64_t rr = s_ubase[own[r]] + static_cast<uint64_t>(idx - static_cast<int>(s_wpfx[own[r]]));
-                    tp.u_idx[rr] = outside[r] ? kNoStall : static_cast<uint32_t>(term[r]);
+                    // pair members (handled by the pair records) and terms outside the len_k set (not
+                    // scaled) get the "skip" index, so the reverse step needs no done bits
+                    tp.u_idx[rr] = skip[r] ? kNoStall : static_cast<uint32_t>(term[r]);
                     tp.u_val[rr] = vv[r];
                 }
                 if (!skip[r] && (last == nullptr || last[term[r]] >= static_cast<int32_t>(step)))
