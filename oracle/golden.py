@@ -121,13 +121,22 @@ def _batch_instance(depth: int):
     return next(wl for wl in W.batch_ising50(256) if wl.extra["depth"] == depth)
 
 
-#: full-depth workloads whose final stores are too large to keep in full (up to ~5e7 terms): only a
+def _line20_schrodinger():
+    """The full 20-qubit line circuit in the Schrodinger picture, schrodinger_cutoff 4 (6.4e7 final terms)."""
+    import dataclasses
+
+    wl = W.line20()
+    return dataclasses.replace(wl, extra={**wl.extra, "schrodinger_cutoff": 4})
+
+
+#: full-depth workloads whose final stores are too large to keep in full (up to ~6.4e7 terms): only a
 #: bucketed digest is committed (``full_<name>.npz``). name -> zero-argument workload builder.
 FULL_DEPTH = {
     "ising100": W.ising100,
     "hubbard6x6": W.hubbard6x6,
     "ising50_b24": lambda: _batch_instance(24),
     "ising50_b12": lambda: _batch_instance(12),
+    "line20_s4": _line20_schrodinger,
 }
 
 DIGEST_BUCKETS = 2048

@@ -126,10 +126,12 @@ def fixture_workload(name: str, reference_root: str, lower_atol=None):
     return wl, float(d["actual_energy"]), np.asarray(d["actual_gradient"], dtype=np.float64)
 
 
-def full_depth() -> None:
-    """Digests of the full-depth circuits, propagated by the reference with one partition (its raw
-    export needs the whole store in one partition)."""
+def full_depth(names=None) -> None:
+    """Digests of the full-depth circuits (all, or ``names``), propagated by the reference with one
+    partition (its raw export needs the whole store in one partition)."""
     for name, make in golden.FULL_DEPTH.items():
+        if names and name not in names:
+            continue
         wl = make()
         r = oracle.run_ref(wl)
         d = golden.bucket_digest(r.keys, r.coefs)
@@ -204,8 +206,9 @@ def main(reference_root: str | None = None) -> None:
     oracle.build(reference_root)
     if not oracle.ref_available():
         raise SystemExit("reference oracle could not be built")
-    if "--full-depth" in sys.argv:
-        full_depth()
+    full = [a for a in sys.argv if a == "--full-depth" or a.startswith("--full-depth=")]
+    if full:  # --full-depth (all) or --full-depth=name,name
+        full_depth(full[0].split("=", 1)[1].split(",") if "=" in full[0] else None)
         return
     if "--surface" in sys.argv:
         surface(reference_root)

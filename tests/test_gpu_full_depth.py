@@ -10,7 +10,9 @@ largest coefficients term by term (1e-10 relative), and <0|O|0> (1e-10 relative)
 * the 100-qubit kicked Ising circuit (5600 gates, Pauli weight <= 10, lower_atol 1e-5): ~3.1e7 terms;
 * the 6x6 spinful Hubbard circuit (2208 gates, Majorana length <= 8, lower_atol 1e-5);
 * two instances of the batched 50-qubit workload, depths 24 and 12 (Pauli weight <= 8), through a plain
-  engine and, for the depth-12 one, through the batch runner with an export per instance.
+  engine and, for the depth-12 one, through the batch runner with an export per instance;
+* the 20-qubit line circuit (390 gates) in the Schrodinger picture with schrodinger_cutoff 4: the
+  evolved state's ~6.4e7 paired monomials.
 """
 
 import numpy as np
