@@ -51,11 +51,18 @@ constexpr int kSweepBlocksPerSM = MPX_SWEEP_BLOCKS;
 #ifndef MPX_SWEEP_BATCH
 #define MPX_SWEEP_BATCH 8
 #endif
+// Column words per interleave unit of a chunk (a divisor of 32). Measured on the 100-qubit circuit:
+// 32 (whole chunks) 227 ms, 8 215 ms, 4 213.5 ms, 1 242 ms per propagate.
+#ifndef MPX_SWEEP_UNIT
+#define MPX_SWEEP_UNIT 4
+#endif
 constexpr int kPrefetch = MPX_SWEEP_PREFETCH;
 constexpr int kBatch = MPX_SWEEP_BATCH;
+constexpr int kUnitWords = MPX_SWEEP_UNIT;
+static_assert(kUnitWords >= 1 && kUnitWords <= 32 && 32 % kUnitWords == 0, "interleave unit must divide 32");
 
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
-// warp w of block b scans the 1024-term chunks b + grid * (w + warps * i); block b owns the query
+// warp w of block b scans the chunks b + grid * (w + warps * i) of 1024 terms each; block b owns the query
 // region [b * warps * stride, (b + 1) * warps * stride), at least as many slots as its warps scan terms.
 struct SweepGeometry {
     uint64_t nwords, nchunks, stride;
@@ -69,6 +76,17 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
     g.n_warps = gridDim.x * kWarps;
     g.stride = ((g.nchunks + g.n_warps - 1) / g.n_warps) * 1024;
     return g;
+}
+
+// The column word that lane `lane` of chunk c scans. A chunk is 32 / kUnitWords units of kUnitWords
+// consecutive words, and unit u of chunk c is word range [(c + u * nchunks) * kUnitWords, + kUnitWords):
+// consecutive units of the store belong to consecutive chunks, hence to consecutive blocks. Anticommuting
+// terms cluster in index ranges (one gate's appends tend to anticommute with the next gate); with whole
+// 1024-term chunks a cluster loads the few blocks that own it, with 128-term units it spreads over
+// eight times as many. (c, lane) -> word is a bijection of [0, nchunks) x [0, 32) onto [0, 32 nchunks).
+__device__ __forceinline__ uint64_t chunk_word(uint64_t c, int lane, uint64_t nchunks) {
+    return (c + static_cast<uint64_t>(lane / kUnitWords) * nchunks) * kUnitWords +
+           static_cast<uint64_t>(lane % kUnitWords);
 }
 
 // Fused anticommutation scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
@@ -160,7 +178,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
             int total = 0;
 #pragma unroll 2
             for (int b = 0; b < nb; ++b) {
-                const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+                const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
                 uint32_t anti = 0, foll = 0;
                 if (j < geo.nwords) {
                     if (n_fold <= kMaxFoldCols) {
@@ -239,7 +257,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                         loc[r] = ow * (kBatch * 1024) + l;
                         const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
                                                static_cast<uint64_t>(lo >> 5) * geo.n_warps;
-                        vv[r] = st.coef[chunk * 1024 + static_cast<uint64_t>(l & 1023)];
+                        vv[r] = st.coef[chunk_word(chunk, lo & 31, geo.nchunks) * 32 + static_cast<uint64_t>(l & 31)];
                     }
                 }
 #pragma unroll
@@ -250,9 +268,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                     const int ow = L < 0 ? 0 : (L / (kBatch * 1024));
                     const int l = L < 0 ? 0 : (L % (kBatch * 1024));
                     const int word = l >> 5; // batch word: chunk (word >> 5), lane (word & 31)
-                    const uint64_t term = (it0 + static_cast<uint64_t>(gridDim.x) * ow +
-                                           static_cast<uint64_t>(word >> 5) * geo.n_warps) * 1024 +
-                                          static_cast<uint64_t>(l & 1023);
+                    const uint64_t term = chunk_word(it0 + static_cast<uint64_t>(gridDim.x) * ow +
+                                                         static_cast<uint64_t>(word >> 5) * geo.n_warps,
+                                                     word & 31, geo.nchunks) * 32 +
+                                          static_cast<uint64_t>(l & 31);
                     bool emit = false, follower = false;
                     int phase = 0;
                     bool member = L >= 0;
@@ -323,7 +342,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
             }
             __syncthreads(); // every round of this batch is done: the emit bitmaps are final
             for (int b = 0; b < nb; ++b) {
-                const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+                const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
                 if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][b * 32 + lane];
             }
             anti_count += static_cast<uint32_t>(total);
@@ -404,7 +423,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
         int total = 0;
 #pragma unroll 2
         for (int b = 0; b < nb; ++b) {
-            const uint64_t j = (c0 + static_cast<uint64_t>(b) * geo.n_warps) * 32 + lane;
+            const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
             uint32_t anti = 0, dn = 0, lg = 0; // lg: terms outside the only_rotate_len_k set
             if (j < geo.nwords) {
                 if (n_fold <= kMaxFoldCols) {
@@ -487,7 +506,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                     const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
                                            static_cast<uint64_t>(lo >> 5) * geo.n_warps;
                     own[r] = ow;
-                    term[r] = chunk * 1024 + static_cast<uint64_t>(lo & 31) * 32 + bit;
+                    term[r] = chunk_word(chunk, lo & 31, geo.nchunks) * 32 + bit;
                     outside[r] = (s_long[ow][lo] >> bit) & 1u;
                     skip[r] = ((s_done[ow][lo] >> bit) & 1u) || outside[r];
                     vv[r] = st.coef[term[r]];
