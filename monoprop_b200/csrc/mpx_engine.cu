@@ -397,18 +397,6 @@ void launch_dep(mpx_engine *e, void (*kernel)(KArgs...), Args... args) {
 
 template <int W, int B, int EXT>
 void launch_gate_ext(mpx_engine *e, const GateDesc *d_desc, uint32_t gate, uint32_t step, cudaEvent_t *ev) {
-#if defined(MPX_CARVEOUT)
-    // build-time tuning (nvcc -DMPX_CARVEOUT=<percent>): the shared-memory share of the L1/shared split
-    // requested for the per-gate kernels; unset, the driver picks it per launch
-    static const bool carveout_set = [] {
-        cudaFuncSetAttribute(&k_sweep<W, B, false, EXT>, cudaFuncAttributePreferredSharedMemoryCarveout, MPX_CARVEOUT);
-        cudaFuncSetAttribute(&k_resolve<W, B, false, (EXT & 1) != 0>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             MPX_CARVEOUT);
-        cudaGetLastError();
-        return true;
-    }();
-    (void)carveout_set;
-#endif
     if (ev) cudaEventRecord(ev[0], e->stream);
     launch_dep(e, &k_sweep<W, B, false, EXT>, e->st, e->sc, e->d_cnt, d_desc, gate, step, e->tr, e->fwd_tape,
                e->d_stats);
