@@ -64,17 +64,20 @@ static_assert(kUnitWords >= 1 && kUnitWords <= 32 && 32 % kUnitWords == 0, "inte
 // Geometry shared by the sweep and resolve launches of one gate (both use the engine's fixed grid):
 // warp w of block b scans the chunks b + grid * (w + warps * i) of 1024 terms each; block b owns the query
 // region [b * warps * stride, (b + 1) * warps * stride), at least as many slots as its warps scan terms.
+// Term, word and chunk indices are 32-bit: a term index is below 2^32 (the store's capacity limit), so a
+// column word index is below 2^27 and a chunk index below 2^22. Query positions stay 64-bit.
 struct SweepGeometry {
-    uint64_t nwords, nchunks, stride;
+    uint32_t nwords, nchunks;
+    uint64_t stride;
     uint32_t n_warps;
 };
 
 __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
     SweepGeometry g;
-    g.nwords = (n0 + 31) >> 5;
+    g.nwords = static_cast<uint32_t>((n0 + 31) >> 5);
     g.nchunks = (g.nwords + 31) >> 5;
     g.n_warps = gridDim.x * kWarps;
-    g.stride = ((g.nchunks + g.n_warps - 1) / g.n_warps) * 1024;
+    g.stride = static_cast<uint64_t>((g.nchunks + g.n_warps - 1) / g.n_warps) * 1024;
     return g;
 }
 
@@ -84,9 +87,9 @@ __device__ __forceinline__ SweepGeometry sweep_geometry(uint64_t n0) {
 // terms cluster in index ranges (one gate's appends tend to anticommute with the next gate); with whole
 // 1024-term chunks a cluster loads the few blocks that own it, with 128-term units it spreads over
 // eight times as many. (c, lane) -> word is a bijection of [0, nchunks) x [0, 32) onto [0, 32 nchunks).
-__device__ __forceinline__ uint64_t chunk_word(uint64_t c, int lane, uint64_t nchunks) {
-    return (c + static_cast<uint64_t>(lane / kUnitWords) * nchunks) * kUnitWords +
-           static_cast<uint64_t>(lane % kUnitWords);
+__device__ __forceinline__ uint32_t chunk_word(uint32_t c, int lane, uint32_t nchunks) {
+    return (c + static_cast<uint32_t>(lane / kUnitWords) * nchunks) * kUnitWords +
+           static_cast<uint32_t>(lane % kUnitWords);
 }
 
 // Fused anticommutation scan + cos sweep + emit (Scan.h:193-396 with the fused sweep of Scan.h:343-358).
@@ -161,24 +164,24 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
         const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
         const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
         const uint64_t qbase = static_cast<uint64_t>(blockIdx.x) * kWarps * geo.stride;
-        const uint64_t span = static_cast<uint64_t>(kBatch) * geo.n_warps;
+        const uint32_t span = static_cast<uint32_t>(kBatch) * geo.n_warps;
 
         // Consecutive chunks go to consecutive blocks (warp w of block b takes chunks
         // b + grid * (w + warps * i)), so dense index ranges spread over all blocks. Each warp takes its
         // chunks in batches of kBatch (the column loads of the whole batch in flight together); per block
         // iteration, the anticommuting terms of the block's batches form one list in (warp, chunk, lane,
         // bit) order, dealt out in rounds of kBlock * kPrefetch.
-        for (uint64_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
-            const uint64_t c0 = it0 + static_cast<uint64_t>(gridDim.x) * warp;
+        for (uint32_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
+            const uint32_t c0 = it0 + gridDim.x * static_cast<uint32_t>(warp);
             int nb = 0;
             if (c0 < geo.nchunks) {
-                const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
-                nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+                const uint32_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
+                nb = static_cast<int>(left < static_cast<uint32_t>(kBatch) ? left : kBatch);
             }
             int total = 0;
 #pragma unroll 2
             for (int b = 0; b < nb; ++b) {
-                const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
+                const uint32_t j = chunk_word(c0 + static_cast<uint32_t>(b) * geo.n_warps, lane, geo.nchunks);
                 uint32_t anti = 0, foll = 0;
                 if (j < geo.nwords) {
                     if (n_fold <= kMaxFoldCols) {
@@ -255,9 +258,9 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                         }
                         const int l = lo * 32 + nth_set_bit(s_anti[ow][lo], li - static_cast<int>(s_pfx[ow][lo]));
                         loc[r] = ow * (kBatch * 1024) + l;
-                        const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
-                                               static_cast<uint64_t>(lo >> 5) * geo.n_warps;
-                        vv[r] = st.coef[chunk_word(chunk, lo & 31, geo.nchunks) * 32 + static_cast<uint64_t>(l & 31)];
+                        const uint32_t chunk = it0 + gridDim.x * static_cast<uint32_t>(ow) +
+                                               static_cast<uint32_t>(lo >> 5) * geo.n_warps;
+                        vv[r] = st.coef[chunk_word(chunk, lo & 31, geo.nchunks) * 32 + static_cast<uint32_t>(l & 31)];
                     }
                 }
 #pragma unroll
@@ -268,10 +271,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                     const int ow = L < 0 ? 0 : (L / (kBatch * 1024));
                     const int l = L < 0 ? 0 : (L % (kBatch * 1024));
                     const int word = l >> 5; // batch word: chunk (word >> 5), lane (word & 31)
-                    const uint64_t term = chunk_word(it0 + static_cast<uint64_t>(gridDim.x) * ow +
-                                                         static_cast<uint64_t>(word >> 5) * geo.n_warps,
+                    const uint32_t term = chunk_word(it0 + gridDim.x * static_cast<uint32_t>(ow) +
+                                                         static_cast<uint32_t>(word >> 5) * geo.n_warps,
                                                      word & 31, geo.nchunks) * 32 +
-                                          static_cast<uint64_t>(l & 31);
+                                          static_cast<uint32_t>(l & 31);
                     bool emit = false, follower = false;
                     int phase = 0;
                     bool member = L >= 0;
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
             }
             __syncthreads(); // every round of this batch is done: the emit bitmaps are final
             for (int b = 0; b < nb; ++b) {
-                const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
+                const uint32_t j = chunk_word(c0 + static_cast<uint32_t>(b) * geo.n_warps, lane, geo.nchunks);
                 if (j < geo.nwords) sc.emit_bits[j] = s_emit[warp][b * 32 + lane];
             }
             anti_count += static_cast<uint32_t>(total);
@@ -412,18 +415,18 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
     const double C = gd.cosv;
     const uint32_t *__restrict__ parity = st.cols + static_cast<uint64_t>(64 * W) * st.cstride;
     const uint32_t tail = (n0 & 31) ? ((1u << (n0 & 31)) - 1u) : 0xFFFFFFFFu;
-    const uint64_t span = static_cast<uint64_t>(kBatch) * geo.n_warps;
-    for (uint64_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
-        const uint64_t c0 = it0 + static_cast<uint64_t>(gridDim.x) * warp;
+    const uint32_t span = static_cast<uint32_t>(kBatch) * geo.n_warps;
+    for (uint32_t it0 = blockIdx.x; it0 < geo.nchunks; it0 += span) { // block-uniform
+        const uint32_t c0 = it0 + gridDim.x * static_cast<uint32_t>(warp);
         int nb = 0;
         if (c0 < geo.nchunks) {
-            const uint64_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
-            nb = static_cast<int>(left < static_cast<uint64_t>(kBatch) ? left : kBatch);
+            const uint32_t left = (geo.nchunks - c0 + geo.n_warps - 1) / geo.n_warps;
+            nb = static_cast<int>(left < static_cast<uint32_t>(kBatch) ? left : kBatch);
         }
         int total = 0;
 #pragma unroll 2
         for (int b = 0; b < nb; ++b) {
-            const uint64_t j = chunk_word(c0 + static_cast<uint64_t>(b) * geo.n_warps, lane, geo.nchunks);
+            const uint32_t j = chunk_word(c0 + static_cast<uint32_t>(b) * geo.n_warps, lane, geo.nchunks);
             uint32_t anti = 0, dn = 0, lg = 0; // lg: terms outside the only_rotate_len_k set
             if (j < geo.nwords) {
                 if (n_fold <= kMaxFoldCols) {
@@ -479,7 +482,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
         __syncthreads();
         const int btotal = static_cast<int>(s_wpfx[kWarps]);
         for (int k = 0; k < btotal; k += kBlock * kPrefetch) {
-            uint64_t term[kPrefetch];
+            uint32_t term[kPrefetch];
             double vv[kPrefetch];
             int own[kPrefetch];
             bool skip[kPrefetch], outside[kPrefetch];
@@ -503,8 +506,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM)
                         else hi = mid;
                     }
                     const int bit = nth_set_bit(s_anti[ow][lo], li - static_cast<int>(s_pfx[ow][lo]));
-                    const uint64_t chunk = it0 + static_cast<uint64_t>(gridDim.x) * ow +
-                                           static_cast<uint64_t>(lo >> 5) * geo.n_warps;
+                    const uint32_t chunk = it0 + gridDim.x * static_cast<uint32_t>(ow) +
+                                           static_cast<uint32_t>(lo >> 5) * geo.n_warps;
                     own[r] = ow;
                     term[r] = chunk_word(chunk, lo & 31, geo.nchunks) * 32 + bit;
                     outside[r] = (s_long[ow][lo] >> bit) & 1u;
@@ -560,6 +563,17 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
     const GateDesc &gd = gates[gate];
     const bool empty = gd.empty != 0;
     pdl_wait();
+    // Thread t owns regions [t*per, (t+1)*per) of the prefix below. Their query counts are loaded together
+    // with the counters (neither depends on the other) and kept in registers for both passes.
+    const uint32_t G = gridDim.x;
+    const uint32_t per = (G + kBlock - 1) / kBlock;
+    constexpr uint32_t kPer = (kMaxGrid + kBlock - 1) / kBlock;
+    uint32_t qc[kPer];
+#pragma unroll
+    for (uint32_t i = 0; i < kPer; ++i) {
+        const uint32_t r = threadIdx.x * per + i;
+        qc[i] = (i < per && r < G) ? sc.blk_q[r] : 0u;
+    }
     const uint32_t stall = cnt->stall;
     const uint64_t n0 = cnt->n0;
     if (stall != kNoStall) return;
@@ -567,11 +581,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
     const uint32_t lt_mask = (1u << lane) - 1u;
     const SweepGeometry geo = sweep_geometry(n0);
     if (empty || n0 == 0) return;
-    // prefix of the per-region counts: thread t owns regions [t*per, (t+1)*per)
-    const uint32_t G = gridDim.x;
-    const uint32_t per = (G + kBlock - 1) / kBlock;
+    // prefix of the per-region counts
     uint32_t mine = 0;
-    for (uint32_t r = threadIdx.x * per; r < (threadIdx.x + 1) * per && r < G; ++r) mine += sc.blk_q[r];
+#pragma unroll
+    for (uint32_t i = 0; i < kPer; ++i) mine += qc[i];
     uint32_t incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -585,9 +598,13 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
     for (int w = 0; w < kWarps; ++w) wbase += (w < warp) ? s_wsum[w] : 0u;
     {
         uint32_t acc = wbase + incl - mine;
-        for (uint32_t r = threadIdx.x * per; r < (threadIdx.x + 1) * per && r < G; ++r) {
-            s_pfx[r] = acc;
-            acc += sc.blk_q[r];
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) {
+            const uint32_t r = threadIdx.x * per + i;
+            if (i < per && r < G) {
+                s_pfx[r] = acc;
+                acc += qc[i];
+            }
         }
     }
     uint32_t Q = 0;
@@ -615,6 +632,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
         uint32_t tag = 0, src = 0, tgt = 0;
         int8_t code = 0;
         double v = 0.0, ph = 0.0, vt = 0.0;
+        double cs = 0.0, cf = 0.0, ax = 0.0; // source, partner and partner's kept pre-gate value
+        uint32_t ebw = 0;                    // the partner's word of the leader-emitted bitmap
         if (k < hi) {
             // region of query k: the last r with s_pfx[r] <= k
             uint32_t a = 0, b = G;
@@ -624,15 +643,24 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                 else b = mid;
             }
             const uint64_t q = a * region_slots + (k - s_pfx[a]);
+            // The source's coefficient (for a rotation) is loaded alongside its key; the candidate's key,
+            // coefficient and leader bit are loaded together below (measured: a hash carried in the
+            // query record instead, sparing the source-key load, made the sweep's emits dearer and the
+            // whole propagate 2% slower).
             src = sc.q_src[q];
             const uint8_t flag = sc.q_flag[q];
             v = sc.q_val[q];
             ph = phase_value(static_cast<uint8_t>(flag >> 1));
             uint64_t m[W];
             load_key<W>(st.keys, src, m); // mostly an L2 hit: the sweep has just read this row
+            cs = st.coef[src];
+            uint64_t h;
+            {
+                uint64_t pp[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) p[w] = m[w] ^ g[w];
-            const uint64_t h = key_hash<W>(p);
+                for (int w = 0; w < W; ++w) pp[w] = m[w] ^ g[w];
+                h = key_hash<W>(pp);
+            }
             tag = static_cast<uint32_t>(h >> 32);
             pos = h & st.tmask;
             uint64_t found = ~0ULL;
@@ -653,11 +681,19 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                 if ((REPLAY || idx < n0) && static_cast<uint32_t>(slot >> 32) == tag) {
                     uint64_t o[W];
                     load_key<W>(st.keys, idx, o);
+                    // what a hit needs, loaded together with the candidate key (a matching tag is almost
+                    // always the partner; the values are dropped otherwise)
+                    const double cf_c = st.coef[idx];
+                    const uint32_t eb_c = sc.emit_bits[idx >> 5];
+                    const double ax_c = (LENK || cos_zero) ? sc.aux[idx] : 0.0;
                     bool eq = true;
 #pragma unroll
-                    for (int w = 0; w < W; ++w) eq = eq && (o[w] == p[w]);
+                    for (int w = 0; w < W; ++w) eq = eq && (o[w] == (m[w] ^ g[w]));
                     if (eq) {
                         found = idx;
+                        cf = cf_c;
+                        ebw = eb_c;
+                        ax = ax_c;
 #pragma unroll
                         for (int w = 0; w < W; ++w) fpop += __popcll(o[w]);
                         break;
@@ -665,6 +701,8 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                 }
                 pos = (pos + 1) & st.tmask;
             }
+#pragma unroll
+            for (int w = 0; w < W; ++w) p[w] = m[w] ^ g[w];
             if constexpr (REPLAY) {
                 if (miss) { // the forward pass found or appended every partner of this gate
                     atomicOr(&cnt->err, 8u);
@@ -681,14 +719,16 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
             }
             if (!miss && !gave_up) {
                 const bool follower = (flag & 1) != 0;
-                const bool leader_took_it = follower && ((sc.emit_bits[found >> 5] >> (found & 31)) & 1u);
+                const bool leader_took_it = follower && ((ebw >> (found & 31)) & 1u);
                 if (!leader_took_it) {
+                    // cs and cf are the current values of both slots: each slot of a pair is written by the
+                    // one thread that rotates the pair (src != found: G is not the identity)
                     if constexpr (LENK) // pre-gate value: kept by the sweep, or untouched (partner outside the cos set)
-                        vt = fpop <= static_cast<int>(tr.len_k) ? sc.aux[found] : st.coef[found];
+                        vt = fpop <= static_cast<int>(tr.len_k) ? ax : cf;
                     else
-                        vt = cos_zero ? sc.aux[found] : st.coef[found] * inv_cos;
-                    st.coef[src] = __fma_rn(sinv * -ph, vt, st.coef[src]);
-                    st.coef[found] = __fma_rn(sinv * ph, v, st.coef[found]);
+                        vt = cos_zero ? ax : cf * inv_cos;
+                    st.coef[src] = __fma_rn(sinv * -ph, vt, cs);
+                    st.coef[found] = __fma_rn(sinv * ph, v, cf);
                     rec = true; // a rotated pair (recorded in replay mode and by a recording forward pass)
                     tgt = static_cast<uint32_t>(found);
                     code = static_cast<int8_t>(static_cast<int>(ph) & 0xF);
@@ -732,7 +772,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                 // Schrodinger (FusedApply.h:39-83): the new slot starts from its reference-state score vt,
                 // and the pair rotates as a hit does (the source's cos factor is already applied)
                 const double vt0 = state_score<W, BASIS>(p, tr.occ);
-                st.coef[src] = __fma_rn(sinv * -ph, vt0, st.coef[src]);
+                st.coef[src] = __fma_rn(sinv * -ph, vt0, cs);
                 c_new = (!cos_zero && !LENK) ? __fma_rn(gd.cosv, vt0, (sinv * ph) * v)
                                              : __fma_rn(sinv * ph, v, gd.cosv * vt0);
             }
