@@ -62,7 +62,10 @@ typedef struct {
      * ceil(min(schrodinger_cutoff, 2 * logical modes) / 2) mode pairs over the logical modes, each holding its
      * reference-state score (generate_paired_op, MajoranaAlgebra.h:127-160); the observable is kept apart,
      * gates run first to last at the negated angle, an appended partner starts from its score
-     * (FusedApply.h:39-83), and <O> = core + observable . state (MPFunctions.cpp:196-205). */
+     * (FusedApply.h:39-83), and <O> = core + observable . state (MPFunctions.cpp:196-205). Graphs replay
+     * from the dense reference state (every stored term at its score), the adjoint starts from the
+     * observable, paring keeps the observable's terms above the threshold, and gradients are returned per
+     * circuit layer as in the Heisenberg picture. */
     int32_t has_schrodinger;
     int32_t schrodinger_cutoff;
     int32_t logical_num_modes; /* modes the paired initial state spans (0 = num_modes) */

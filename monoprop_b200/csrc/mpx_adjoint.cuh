@@ -329,7 +329,9 @@ struct Frozen {
     // (-1: never); a step skips the cos scaling of a term with last < step and the rotation of a pair with
     // both endpoints below it. nullptr: no paring.
     const int32_t *last;
-    // only_rotate_len_k of the build: one bit per term of more than k slots (never cos-scaled); nullptr: none
+    // only_rotate_len_k of a recorded propagation: one bit per term of more than k slots (never cos-scaled,
+    // and a pair's partner among them keeps no cos factor, code 0x20); nullptr: every anticommuting term is
+    // scaled and 0x20 is ignored (a built graph, as the reference replays it)
     const uint32_t *longb;
 };
 
@@ -357,6 +359,16 @@ __global__ void __launch_bounds__(kBlock) k_pare_init(const uint64_t *__restrict
         for (int w = 0; w < W; ++w) unpaired |= (m[w] & kEven) ^ ((m[w] >> 1) & kEven);
         last[i] = (unpaired == 0 && keep_paired) ? last_step : -1;
     }
+}
+
+// Schrodinger picture: the kept terms after the last step are the observable's terms whose |coefficient|
+// exceeds the threshold (indices_above on the driving vector, MonomialPropagator.inl:960-962); `last` is
+// -1 everywhere else. idx[t] = kNoStall for an observable term the store does not hold.
+__global__ void k_pare_seed(const uint32_t *__restrict__ idx, const double *__restrict__ val, uint64_t n,
+                            double threshold, int32_t last_step, int32_t *__restrict__ last) {
+    for (uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; t < n;
+         t += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        if (idx[t] != kNoStall && fabs(val[t]) > threshold) last[idx[t]] = last_step;
 }
 
 // One step, backward: a pair with an endpoint still relevant after the step makes both endpoints relevant
@@ -392,10 +404,16 @@ __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ co
         const int8_t code = fz.code[b + k];
         const bool appended = (code & 0x10) != 0;
         const double phi = static_cast<double>(static_cast<int8_t>(code << 4) >> 4);
-        const double vs = coef[s], vt = appended ? 0.0 : coef[t];
+        // An appended partner's slot still holds the value the replay started it from (no earlier gate
+        // reaches a term created later): 0 in the Heisenberg picture, the reference-state score in the
+        // Schrodinger picture. The reference's replay scales it by cos like every anticommuting term below
+        // the post-insert count and adds the sine term (Evolution.cpp:471-511, Engine.h:628-633).
+        const double vs = coef[s], vt = coef[t];
         const bool pared = fz.last != nullptr && fz.last[s] < static_cast<int32_t>(step) &&
                            fz.last[t] < static_cast<int32_t>(step);
-        const bool unscaled_t = (code & 0x20) != 0; // partner outside the only_rotate_len_k set
+        // partner outside the only_rotate_len_k set: unscaled in the adjoint of a propagation (longb given);
+        // a built graph scales it as any anticommuting term
+        const bool unscaled_t = (code & 0x20) != 0 && fz.longb != nullptr;
         if (!pared) {
             coef[s] = C * vs - S * phi * vt;
             coef[t] = (unscaled_t ? vt : C * vt) + S * phi * vs;
@@ -406,7 +424,7 @@ __global__ void __launch_bounds__(kBlock) k_frozen_pairs(double *__restrict__ co
             const uint64_t r = tp.p_base[step] + k;
             tp.p_src[r] = s;
             tp.p_tgt[r] = t;
-            tp.p_code[r] = code;
+            tp.p_code[r] = unscaled_t ? code : static_cast<int8_t>(code & ~0x20);
             tp.p_vs[r] = vs;
             tp.p_vt[r] = vt;
         }

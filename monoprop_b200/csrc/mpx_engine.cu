@@ -85,7 +85,15 @@ struct FrozenGraph {
     double last_for = -1.0;                 // threshold `last` was computed for (< 0: none yet)
     // the device view the frozen kernels take
     uint32_t *longb = nullptr;              // only_rotate_len_k of the build: terms outside its set (bits)
-    Frozen view() const { return Frozen{src, tgt, code, p_begin, p_count, pared ? last : nullptr, longb}; }
+    // A built graph replays as the reference's graph does: its cos set is recomputed from the fold over all
+    // terms below the post-insert count, with no length filter (MonomialPropagator.inl:872-895), so terms
+    // outside the only_rotate_len_k set are scaled there and a pair's partner outside it is a plain pair.
+    // The recorded view of a propagation (the adjoint of that propagation) keeps the forward semantics:
+    // such terms and partners are never scaled.
+    bool forward_len_k = false;
+    Frozen view() const {
+        return Frozen{src, tgt, code, p_begin, p_count, pared ? last : nullptr, forward_len_k ? longb : nullptr};
+    }
 };
 
 struct mpx_engine {
@@ -507,10 +515,13 @@ FrozenFn pick_frozen(int W) {
     }
 }
 
+// out[i] = the reference-state score of stored term i, for i in [lo, hi)
 template <int W, int B>
-void launch_adj_init(mpx_engine *e, double *lam, uint64_t n) {
+void launch_adj_init(mpx_engine *e, double *out, uint64_t lo, uint64_t hi) {
+    const uint64_t n = hi - lo;
     const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock + 1, static_cast<uint64_t>(e->grid) * 4);
-    k_adj_init<W, B><<<static_cast<unsigned>(blocks), kBlock, 0, e->stream>>>(e->st.keys, n, e->mask, lam);
+    k_adj_init<W, B><<<static_cast<unsigned>(blocks), kBlock, 0, e->stream>>>(e->st.keys + lo * W, n, e->mask,
+                                                                              out + lo);
 }
 
 template <int W, int B>
@@ -537,7 +548,7 @@ void launch_build(mpx_engine *e, uint64_t lo, uint64_t hi) {
 
 using GateFn = void (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t);
 using ReplayFn = void (*)(mpx_engine *, const GateDesc *, uint32_t, uint32_t, const Tape &);
-using AdjInitFn = void (*)(mpx_engine *, double *, uint64_t);
+using AdjInitFn = void (*)(mpx_engine *, double *, uint64_t, uint64_t);
 using ExpFn = void (*)(mpx_engine *);
 using BuildFn = void (*)(mpx_engine *, uint64_t, uint64_t);
 
@@ -1202,6 +1213,27 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
     return MPX_OK;
 }
 
+// Values the replay starts terms [lo, hi) of the final store from: the reference-state score in the
+// Schrodinger picture; otherwise 0, and with `with_start` the re-weighted initial operator's terms in that
+// range (mpx_update_initial_operator; frozen_forward starts from them). A segment's checkpoint holds the
+// terms that existed at its start; the frozen pair kernel reads an appended partner's slot at its gate, so
+// the later slots must hold these values again before the segment is replayed.
+mpx_status replay_start_tail(mpx_engine *eng, uint64_t lo, uint64_t hi, bool with_start) {
+    mpx_engine *e = eng;
+    if (hi <= lo) return MPX_OK;
+    if (e->schr) {
+        pick_adj_init(e->W, e->cfg.basis)(e, e->st.coef, lo, hi);
+    }
+    else {
+        MPX_CUDA(cudaMemsetAsync(e->st.coef + lo, 0, (hi - lo) * sizeof(double), e->stream));
+        if (with_start && e->start_on && e->n_start > 0)
+            k_scatter<<<static_cast<unsigned>(std::min<uint64_t>((e->n_start + 255) / 256, 4096)), 256, 0, e->stream>>>(
+                e->st.coef, e->d_start_idx, e->d_start_val, e->n_start, static_cast<uint32_t>(lo));
+    }
+    MPX_CUDA(cudaGetLastError());
+    return MPX_OK;
+}
+
 // Reverse sweep: per segment (last first) restore its checkpoint, replay it logging the tape, then walk
 // its gates backwards. grad_angles[l] = dE/d(angle_l) for circuit layer l (angle = theta[map] * g).
 // With fg == nullptr: the gradient of the last mpx_adjoint_forward (segments replayed with the
@@ -1299,7 +1331,19 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
     MPX_CUDA_REL(cudaMemsetAsync(done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
     const GradPartials gp{gpart, reinterpret_cast<unsigned int *>(gpart + 2 * static_cast<size_t>(e->grid))};
     MPX_CUDA_REL(cudaMemsetAsync(gp.arrivals, 0, sizeof(unsigned int), e->stream));
-    pick_adj_init(e->W, e->cfg.basis)(e, lam, nf);
+    if (e->schr) {
+        // Schrodinger: <O> = core + sum_t o_t state[idx_t], so the adjoint of the final state is the
+        // observable at its terms' store rows (0 elsewhere)
+        MPX_CUDA_REL(cudaMemsetAsync(lam, 0, std::max<uint64_t>(nf, 1) * sizeof(double), e->stream));
+        if (e->n_obs > 0 && nf > 0) {
+            pick_lookup(e->W)(e, e->d_obs_keys, e->n_obs, nf, e->d_obs_idx);
+            k_scatter<<<static_cast<unsigned>(std::min<uint64_t>((e->n_obs + 255) / 256, 4096)), 256, 0, e->stream>>>(
+                lam, e->d_obs_idx, e->d_obs_coef, e->n_obs);
+        }
+    }
+    else {
+        pick_adj_init(e->W, e->cfg.basis)(e, lam, 0, nf);
+    }
     const ReplayFn replay = pick_replay(e->W, e->cfg.basis);
     const FrozenFn frozen_replay = pick_frozen<true>(e->W);
     Frozen fz{};
@@ -1310,6 +1354,13 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         if (n > 0)
             MPX_CUDA_REL(cudaMemcpyAsync(e->st.coef, A.ck_coef[sg], n * sizeof(double), cudaMemcpyDeviceToDevice,
                                          e->stream));
+        if (fg != nullptr && nf > n) {
+            const mpx_status ts = replay_start_tail(e, n, nf, fg == &e->fg);
+            if (ts != MPX_OK) {
+                release();
+                return ts;
+            }
+        }
         Counters c{};
         c.n = n;
         c.n0 = n;
@@ -1383,6 +1434,7 @@ mpx_status recorded_view(mpx_engine *eng, FrozenGraph &v) {
     v.p_begin = A.r_begin;
     v.w_anti = A.w_anti;
     v.longb = A.longb;
+    v.forward_len_k = true;
     v.n0.resize(L);
     v.anti.resize(L);
     v.count.resize(L);
@@ -1427,8 +1479,9 @@ PareInitFn pick_pare_init(int W) {
     }
 }
 
-// Pares the frozen graph against the reference state at `threshold` (the reference's pare_graph,
-// PareGraph.cpp:103-141): last[i] from the scored terms, then one backward step per layer over its pairs.
+// Pares the frozen graph at `threshold` (the reference's pare_graph, PareGraph.cpp:103-141): last[i] from
+// the driving vector (the reference state's scores; in the Schrodinger picture the observable), then one
+// backward step per layer over its pairs.
 mpx_status graph_pare(mpx_engine *eng, double threshold) {
     mpx_engine *e = eng;
     FrozenGraph &g = e->fg;
@@ -1442,8 +1495,20 @@ mpx_status graph_pare(mpx_engine *eng, double threshold) {
     }
     if (g.last == nullptr)
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&g.last), std::max<uint64_t>(g.n_final, 1) * sizeof(int32_t)));
-    // |weight| = 1 on fully paired terms: kept iff 1 > threshold
-    pick_pare_init(e->W)(e, g.n_final, 1.0 > threshold ? 1 : 0, static_cast<int32_t>(g.L) - 1, g.last);
+    if (e->schr) {
+        // Schrodinger: the driving vector is the observable (MonomialPropagator.inl:960-962): its terms
+        // above the threshold are the ones kept after the last step
+        MPX_CUDA(cudaMemsetAsync(g.last, 0xFF, std::max<uint64_t>(g.n_final, 1) * sizeof(int32_t), e->stream));
+        if (e->n_obs > 0 && g.n_final > 0) {
+            pick_lookup(e->W)(e, e->d_obs_keys, e->n_obs, g.n_final, e->d_obs_idx);
+            k_pare_seed<<<static_cast<unsigned>(std::min<uint64_t>((e->n_obs + 255) / 256, 4096)), 256, 0, e->stream>>>(
+                e->d_obs_idx, e->d_obs_coef, e->n_obs, threshold, static_cast<int32_t>(g.L) - 1, g.last);
+        }
+    }
+    else {
+        // |weight| = 1 on fully paired terms: kept iff 1 > threshold
+        pick_pare_init(e->W)(e, g.n_final, 1.0 > threshold ? 1 : 0, static_cast<int32_t>(g.L) - 1, g.last);
+    }
     const Frozen fz = Frozen{g.src, g.tgt, g.code, g.p_begin, g.p_count, nullptr, nullptr};
     for (uint64_t st = g.L; st-- > 0;) {
         const uint64_t cnt = g.count[st];
@@ -1486,6 +1551,7 @@ mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_g
         // The forward pass logged every gate's pairs: the graph takes the log over, no replay needed.
         s = recorded_view(e, g);
         if (s != MPX_OK) return s;
+        g.forward_len_k = false; // a built graph replays as the reference's graph (no length filter)
         g.circuit_id = cd.id;
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&g.done), std::max<uint64_t>((nf + 31) / 32, 4) * sizeof(uint32_t)));
         MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
@@ -1625,7 +1691,12 @@ mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segmen
     FrozenGraph &g = e->fg;
     const uint64_t L = g.L, nf = g.n_final;
     free_adjoint(e);
-    if (e->start_on) {
+    if (e->schr) {
+        // Schrodinger: the replay starts from the dense reference state, every stored term at its
+        // reference-state score, appended terms included (MPOperator.h:169-181)
+        if (nf > 0) pick_adj_init(e->W, e->cfg.basis)(e, e->st.coef, 0, nf);
+    }
+    else if (e->start_on) {
         // the re-weighted initial operator (mpx_update_initial_operator), in store positions
         if (nf > 0) MPX_CUDA(cudaMemsetAsync(e->st.coef, 0, nf * sizeof(double), e->stream));
         if (e->n_start > 0)
@@ -2166,13 +2237,18 @@ mpx_status mpx_graph_replay_count(mpx_engine *e, uint64_t *out) {
     return MPX_OK;
 }
 
+// The Schrodinger picture runs the circuit first to last at negated angles (gate descriptor l is circuit
+// layer L-1-l at -angle): the adjoint's derivatives per descriptor, mapped back to circuit layers.
+void schr_grad_to_layers(const mpx_engine *e, double *grad, uint64_t L) {
+    if (!e->schr || L == 0) return;
+    const std::vector<double> g(grad, grad + L);
+    for (uint64_t l = 0; l < L; ++l) grad[L - 1 - l] = -g[l];
+}
+
 mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation) {
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
-    if (e->schr)
-        return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
-                                        "the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = adjoint_forward(e, *c, segment_gates);
     if (s != MPX_OK) return s;
@@ -2195,6 +2271,7 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
         e->tr.len_k = e->adj.len_k;
         const mpx_status s = adjoint_backward(e, *c, grad_angles);
         e->tr = saved;
+        if (s == MPX_OK) schr_grad_to_layers(e, grad_angles, c->n);
         return s;
     }
     // The forward pass recorded every gate's pairs: replay the segments with the frozen kernels.
@@ -2203,6 +2280,7 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
     if (s != MPX_OK) return s;
     s = adjoint_backward(e, *c, grad_angles, &view);
     dev_free(e, view.p_count);
+    if (s == MPX_OK) schr_grad_to_layers(e, grad_angles, c->n);
     return s;
 }
 
@@ -2210,9 +2288,6 @@ mpx_status mpx_graph_build(mpx_engine *e, const mpx_circuit *c, uint64_t segment
     if (e == nullptr || c == nullptr || expectation == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
-    if (e->schr)
-        return fail(eng, MPX_ERR_STATE, "the Schrodinger picture is supported by propagate and expectation only (not by "
-                                        "the gradient or graph)");
     MPX_CUDA(cudaSetDevice(e->device));
     mpx_status s = graph_build(e, *c, segment_gates);
     if (s != MPX_OK) return s;
@@ -2247,6 +2322,7 @@ mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segm
     s = frozen_forward(e, *c, segment_gates == 0 ? std::max<uint64_t>(c->n, 1) : segment_gates);
     if (s == MPX_OK) s = mpx_expectation(e, expectation);
     if (s == MPX_OK && c->n > 0) s = adjoint_backward(e, *c, grad_angles, &e->fg);
+    if (s == MPX_OK) schr_grad_to_layers(e, grad_angles, c->n);
     e->adj.w_anti = nullptr; // owned by the graph
     free_adjoint(e);
     return s;
@@ -2329,6 +2405,7 @@ mpx_status mpx_update_initial_operator(mpx_engine *e, const uint64_t *words, con
         }
         e->n_obs = n;
         if (has_core) e->core = core;
+        e->fg.last_for = -2.0; // a pared graph's keep set came from the old observable
         MPX_CUDA(cudaStreamSynchronize(e->stream));
         return MPX_OK;
     }

@@ -709,11 +709,20 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                     miss = false;
                 }
                 else if (!gave_up && found >= n0) {
-                    st.coef[found] = (sinv * ph) * v;
+                    // the append of the forward pass, redone with the same arithmetic as its miss branch
+                    // (vt, the partner's value before the gate, goes to the pair log)
+                    vt = 0.0;
+                    double c_new = (sinv * ph) * v;
+                    if (tr.schr) {
+                        vt = state_score<W, BASIS>(p, tr.occ);
+                        st.coef[src] = __fma_rn(sinv * -ph, vt, cs);
+                        c_new = (!cos_zero && !LENK) ? __fma_rn(gd.cosv, vt, (sinv * ph) * v)
+                                                     : __fma_rn(sinv * ph, v, gd.cosv * vt);
+                    }
+                    st.coef[found] = c_new;
                     rec = true;
                     tgt = static_cast<uint32_t>(found);
                     code = static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF));
-                    vt = 0.0;
                     gave_up = true; // handled
                 }
             }
@@ -1010,10 +1019,10 @@ __global__ void k_long_bits(const uint64_t *__restrict__ keys, uint64_t n, uint3
 
 // coef[idx[k]] = val[k] (indices distinct).
 __global__ void k_scatter(double *__restrict__ coef, const uint32_t *__restrict__ idx, const double *__restrict__ val,
-                          uint64_t n) {
+                          uint64_t n, uint32_t lo = 0) {
     for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < n;
          k += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        coef[idx[k]] = val[k];
+        if (idx[k] != kNoStall && idx[k] >= lo) coef[idx[k]] = val[k]; // kNoStall: a term the store does not hold
 }
 
 // <0|O|0>: per-block partial sums over contiguous chunks, fixed-order tree (MPOperator.h:235-254,

@@ -171,6 +171,9 @@ def _load_ref(build: str = "v3") -> C.CDLL:
         lib.mpref_core.argtypes = [C.c_void_p]
         lib.mpref_export.restype = C.c_int64
         lib.mpref_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t]
+        lib.mpref_export_at.restype = C.c_int64
+        lib.mpref_export_at.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.c_char_p, C.c_size_t]
         lib.mpref_destroy.argtypes = [C.c_void_p]
         _ref[build] = lib
     return _ref[build]
@@ -305,13 +308,18 @@ class RefEngine:
     def size(self) -> int:
         return int(self.lib.mpref_size(self.h))
 
-    def export(self) -> tuple[np.ndarray, np.ndarray]:
+    def export(self, params=None) -> tuple[np.ndarray, np.ndarray]:
+        """Raw keys and coefficients of the current operator, or of the stored graph replayed at ``params``."""
         n = self.size()
         W = int(self.lib.mpref_words(self.h))
         keys = np.zeros((max(n, 1), W), dtype=np.uint64)
         coefs = np.zeros(max(n, 1), dtype=np.float64)
         err = C.create_string_buffer(1024)
-        got = self.lib.mpref_export(self.h, _ptr(keys), _ptr(coefs), n, err, 1024)
+        if params is None:
+            got = self.lib.mpref_export(self.h, _ptr(keys), _ptr(coefs), n, err, 1024)
+        else:
+            p = np.ascontiguousarray(params, dtype=np.float64)
+            got = self.lib.mpref_export_at(self.h, p.size, _ptr(p), _ptr(keys), _ptr(coefs), n, err, 1024)
         if got < 0:
             raise RuntimeError(err.value.decode())
         return keys[:got], coefs[:got]

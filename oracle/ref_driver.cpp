@@ -67,7 +67,7 @@ struct Base {
     virtual size_t size() = 0;
     virtual size_t words() = 0;
     virtual double core() = 0;
-    virtual size_t export_terms(uint64_t *words, double *coefs, size_t cap) = 0;
+    virtual size_t export_terms(uint64_t *words, double *coefs, size_t cap, const VecD &params) = 0;
 };
 
 template <size_t N>
@@ -105,8 +105,10 @@ struct Impl final : Base {
     size_t size() override { return p->size(); }
     size_t words() override { return Monomial<N>::num_words(); }
     double core() override { return p->core_term(); }
-    size_t export_terms(uint64_t *words, double *coefs, size_t cap) override {
-        const VecD coeffs = p->contract_partially(VecD{}, false);
+    // the raw coefficients of the current operator (no parameters), or of the stored graph replayed at
+    // `params` (contract_partially(params, false), MonomialPropagator.inl:1053-1097)
+    size_t export_terms(uint64_t *words, double *coefs, size_t cap, const VecD &params) override {
+        const VecD coeffs = p->contract_partially(params, false);
         size_t n = 0;
         constexpr size_t W = Monomial<N>::num_words();
         p->indexing().for_each([&](const auto &mono, size_t idx) {
@@ -261,7 +263,19 @@ double mpref_core(void *h) { return static_cast<Base *>(h)->core(); }
 
 int64_t mpref_export(void *h, uint64_t *words, double *coefs, size_t cap, char *err, size_t errlen) {
     try {
-        return static_cast<int64_t>(static_cast<Base *>(h)->export_terms(words, coefs, cap));
+        return static_cast<int64_t>(static_cast<Base *>(h)->export_terms(words, coefs, cap, VecD{}));
+    }
+    catch (const std::exception &e) {
+        set_err(err, errlen, e.what());
+        return -1;
+    }
+}
+
+int64_t mpref_export_at(void *h, size_t n_params, const double *params, uint64_t *words, double *coefs, size_t cap,
+                        char *err, size_t errlen) {
+    try {
+        return static_cast<int64_t>(
+            static_cast<Base *>(h)->export_terms(words, coefs, cap, VecD(params, params + n_params)));
     }
     catch (const std::exception &e) {
         set_err(err, errlen, e.what());

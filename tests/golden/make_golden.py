@@ -10,7 +10,10 @@ Run in a container that has the reference sources (the GPU hosts do not): it bui
 * ``grad_<workload>.npz`` -- the reference's gradient of the frozen-structure surrogate (graph built with
   the same parameters, then ``expectation_value_and_gradient``), per parameter;
 * ``graph_<workload>.npz`` -- the reference's frozen graph (built at the workload's parameters) replayed
-  at shifted parameters: expectation and gradient there;
+  at shifted parameters: expectation and gradient there (``--graph-len-k``: graphs built with
+  ``only_rotate_len_k``; ``--graph-schrodinger``: graphs in the Schrodinger picture, ``graph_*_s<cutoff>``;
+  ``--graph-replay``: raw coefficients of a len_k graph replayed at its build parameters,
+  ``graph_replay_*``);
 * ``pshift_line20.npz`` -- parameter-shift gradient of the 20-qubit line circuit from the reference's
   replayed graph;
 * ``<workload>_k<k>.npz`` -- seeded workloads propagated with ``only_rotate_len_k = k``;
@@ -173,6 +176,86 @@ def graphs_len_k() -> None:
         print("graph len_k", name, ev0, ev, float(np.abs(grad).max()), float(np.max(np.abs(grad[idx] - fd))))
 
 
+def graph_replays() -> None:
+    """graph_replay_hubbard6x6_L400_k4.npz: the raw coefficients of the reference's graph built with
+    only_rotate_len_k = 4, replayed at its build parameters (contract_partially(params, false)), keys sorted.
+    Its replay recomputes each layer's cos set with no length filter (MonomialPropagator.inl:872-895), so
+    these differ from its own propagation (hubbard6x6_L400_k4.npz) on the terms outside the set and on what
+    they rotate into, while <O> agrees."""
+    wl = dataclasses.replace(W.hubbard6x6(), extra={**W.hubbard6x6().extra, "only_rotate_len_k": 4})
+    L = 400
+    eng = oracle.RefEngine(wl)
+    eng.propagate(n_layers=L, build_graph=True)
+    P = int(wl.param_map[:L].max()) + 1
+    ev = eng.expectation(wl.params[:P])
+    keys, coefs = eng.export(wl.params[:P])
+    eng.close()
+    save_result(os.path.join(HERE, "graph_replay_hubbard6x6_L400_k4.npz"), keys, coefs, ev,
+                {"n_layers": np.int64(L), "only_rotate_len_k": np.int64(4)})
+    print("graph replay hubbard6x6_L400_k4", keys.shape[0], ev)
+
+
+def _schr_fixture(fixture: str, cutoff: int, sc: int, k=None):
+    """The reference's own fermionic test problem ``fixture`` (a ``ref_*`` fixture) in the Schrodinger
+    picture with the given cutoffs, as its gradient test builds it (tests/test_infinite_cutoff.py:72-105,
+    tests/test_only_rotate_k.py:32)."""
+    g = golden.load(fixture)
+    wl = golden.fixture_workload(g, fixture)
+    extra = {**wl.extra, "schrodinger_cutoff": sc}
+    if k is not None:
+        extra["only_rotate_len_k"] = k
+    return dataclasses.replace(wl, cutoff=cutoff, extra=extra), wl.n_layers
+
+
+def _schr_line20(L: int):
+    wl = W.line20()
+    return dataclasses.replace(wl, extra={**wl.extra, "schrodinger_cutoff": 4}), L
+
+
+#: frozen graphs in the Schrodinger picture: name -> zero-argument builder of (workload, layers)
+GRAPHS_SCHR = {
+    "ref_lih_fermionic_spin_exact_c4_s6": lambda: _schr_fixture("ref_lih_fermionic_spin_exact", 4, 6),
+    "ref_lih_fermionic_spin_exact_c6_s8_k4": lambda: _schr_fixture("ref_lih_fermionic_spin_exact", 6, 8, 4),
+    "line20_L200_s4": lambda: _schr_line20(200),
+}
+
+
+def graphs_schrodinger() -> None:
+    """graph_<name>.npz for graphs built in the Schrodinger picture (schrodinger_cutoff, the replay from the
+    dense reference state, MonomialPropagator.inl:1053-1097): the reference's replay at the build parameters
+    and at shifted ones (seed 77, 0.05 N(0, 1)) with its gradient there, plus central finite differences
+    (h = 1e-5) of the replay on up to 16 seeded parameters whose gradient is not zero."""
+    for name, make in GRAPHS_SCHR.items():
+        wl, L = make()
+        eng = oracle.RefEngine(wl)
+        eng.propagate(n_layers=L, build_graph=True)
+        n_params = int(wl.param_map[:L].max()) + 1
+        theta = wl.params[:n_params]
+        shifted = theta + 0.05 * np.random.default_rng(77).standard_normal(n_params)
+        ev, grad, _ = eng.expectation_and_gradient(shifted)
+        ev0 = eng.expectation(theta)
+        live = np.flatnonzero(np.abs(grad) > 1e-9)
+        idx = np.sort(np.random.default_rng(5).choice(live, size=min(16, live.size), replace=False))
+        h = 1e-5
+        fd = np.zeros(idx.size)
+        for j, p in enumerate(idx):
+            tp, tm = shifted.copy(), shifted.copy()
+            tp[p] += h
+            tm[p] -= h
+            fd[j] = (eng.expectation(tp) - eng.expectation(tm)) / (2 * h)
+        size = eng.size()
+        eng.close()
+        extra = {}
+        if wl.extra.get("only_rotate_len_k") is not None:
+            extra["only_rotate_len_k"] = np.int64(wl.extra["only_rotate_len_k"])
+        np.savez_compressed(os.path.join(HERE, f"graph_{name}.npz"), expectation=np.float64(ev),
+                            expectation_build=np.float64(ev0), grad=grad, params=shifted, n_layers=np.int64(L),
+                            schrodinger_cutoff=np.int64(wl.extra["schrodinger_cutoff"]),
+                            cutoff=np.int64(wl.cutoff), terms=np.int64(size), fd_idx=idx, fd=fd, **extra)
+        print("graph schrodinger", name, size, ev0, ev, f"{live.size}/{grad.size} nonzero",
+              float(np.max(np.abs(grad[idx] - fd))) if idx.size else None, flush=True)
+
+
 def surface(reference_root: str) -> None:
     """The names the reference's nanobind module binds per propagator class and module-wide
     (``src/monoprop/bindings/binder.h``, ``bindings.cpp.in``), and the ``_simulator`` attributes its Python
@@ -215,6 +298,12 @@ def main(reference_root: str | None = None) -> None:
         return
     if "--graph-len-k" in sys.argv:
         graphs_len_k()
+        return
+    if "--graph-schrodinger" in sys.argv:
+        graphs_schrodinger()
+        return
+    if "--graph-replay" in sys.argv:
+        graph_replays()
         return
     for name, make, L, k in LEN_K:
         wl = make()

@@ -67,8 +67,8 @@ def test_schrodinger_streaming_from_a_tiny_capacity():
 
 def test_core_schrodinger_surface():
     """The _core class with schrodinger_cutoff: the reference's property, <O> over the evolved state, the
-    observable re-weighted by update_initial_operator, no core term in evolved_operator; the gradient and
-    graph entry points are not offered in this picture."""
+    observable re-weighted by update_initial_operator, no core term in evolved_operator, and a graph built
+    in this picture (its replays are checked in test_gpu_schrodinger_graph.py)."""
     wl, L = golden.schrodinger_workload("hubbard6x6_L200_s4")
     g = golden.load("hubbard6x6_L200_s4")
     obs = {k: complex(v) for k, v in wl.observable.items()}
@@ -86,6 +86,9 @@ def test_core_schrodinger_surface():
     # <O> is linear in the observable: doubling its non-core part doubles <O> - core
     p.update_initial_operator({(): 0.5 + 0j, (0, 1): 1.0j})
     assert abs((p.expectation_value([]) - 0.5) - 2 * (ev - 0.5)) <= 1e-12
-    with pytest.raises(RuntimeError, match="Schrodinger"):
-        p.build_graph([list(m) for m in wl.gate_slots[:10]], list(map(int, wl.param_map[:10])),
-                      list(wl.gen_coeffs[:10]), None, list(wl.params[:int(wl.param_map[:10].max()) + 1]))
+    P10 = int(wl.param_map[:10].max()) + 1
+    p.build_graph([list(m) for m in wl.gate_slots[:10]], list(map(int, wl.param_map[:10])),
+                  list(wl.gen_coeffs[:10]), None, list(wl.params[:P10]))
+    assert p.graph_layers() == 10
+    ev_g, grad = p.expectation_value_and_gradient(list(wl.params[:P10]))
+    assert np.isfinite(ev_g) and len(grad) == P10
