@@ -263,6 +263,11 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                         vv[r] = st.coef[chunk_word(chunk, lo & 31, geo.nchunks) * 32 + static_cast<uint32_t>(l & 31)];
                     }
                 }
+                // Phase 1, every prefetched term: membership, cos scaling, undo log and the lower_atol gate.
+                // Terms that pass the gate are marked (bit r of cand) instead of being finished here: they
+                // are a few per warp (1-10 % of the anticommuting terms), and finishing them in place would
+                // run the key load and the partner, cutoff and phase work once per slot for those few lanes.
+                uint32_t cand = 0;
 #pragma unroll
                 for (int r = 0; r < kPrefetch; ++r) {
                     if (k + kBlock * r + 32 * warp >= btotal) break; // warp-uniform
@@ -275,8 +280,6 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                                                          static_cast<uint32_t>(word >> 5) * geo.n_warps,
                                                      word & 31, geo.nchunks) * 32 +
                                           static_cast<uint32_t>(l & 31);
-                    bool emit = false, follower = false;
-                    int phase = 0;
                     bool member = L >= 0;
                     if ((EXT & 1) && member) {
                         // only_rotate_len_k: a term of more than len_k slots is left alone by this gate
@@ -298,7 +301,6 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                         }
                     }
                     if (member) {
-                        follower = (s_foll[ow][word] >> (l & 31)) & 1u;
                         st.coef[term] = v * cosv;
                         if (cos_zero || (EXT & 1)) sc.aux[term] = v;
                         if constexpr (REPLAY) {
@@ -308,26 +310,76 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                             tp.u_idx[rr] = static_cast<uint32_t>(term);
                             tp.u_val[rr] = v;
                         }
-                        const double av = fabs(v);
-                        if (!(tr.has_lower && sinabs * av <= tr.lower)) {
-                            uint64_t m[W], p[W];
-                            load_key<W>(st.keys, term, m);
-                            int mpop = 0, ov = 0;
+                        if (!(tr.has_lower && sinabs * fabs(v) <= tr.lower)) cand |= 1u << r;
+                    }
+                }
+                // Phase 2: the warp's marked terms, dense, 32 at a time. Candidate c of the warp is slot r_c of
+                // lane src (slots in order, lanes in order within a slot); its location and value come over
+                // by shuffle, so every lane does the key load and the partner work for one real candidate.
+                uint32_t pb[kPrefetch];
+                int pfx[kPrefetch];
+                int n_cand = 0;
 #pragma unroll
-                            for (int w = 0; w < W; ++w) {
-                                const uint64_t gw = gd.g[w];
-                                p[w] = m[w] ^ gw;
-                                mpop += __popcll(m[w]);
-                                ov += __popcll(m[w] & gw);
-                            }
-                            const int ppop = mpop + gpop - 2 * ov;
-                            bool keep;
-                            if constexpr ((EXT & 2) != 0) keep = keep_partner_mapped<W>(p, tr);
-                            else keep = keep_partner<W>(p, ppop, tr);
-                            if (keep || (tr.has_upper && sinabs * av >= tr.upper)) {
-                                emit = true;
-                                phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
-                            }
+                for (int r = 0; r < kPrefetch; ++r) {
+                    pb[r] = __ballot_sync(0xFFFFFFFFu, (cand >> r) & 1u);
+                    pfx[r] = n_cand;
+                    n_cand += __popc(pb[r]);
+                }
+                for (int base = 0; base < n_cand; base += 32) { // warp-uniform
+                    const int ci = base + lane;
+                    int r_c = 0;
+#pragma unroll
+                    for (int r = 1; r < kPrefetch; ++r) r_c += (pfx[r] <= ci) ? 1 : 0;
+                    uint32_t pbr = pb[0];
+#pragma unroll
+                    for (int r = 1; r < kPrefetch; ++r) pbr = (r == r_c) ? pb[r] : pbr;
+                    int pr = pfx[0];
+#pragma unroll
+                    for (int r = 1; r < kPrefetch; ++r) pr = (r == r_c) ? pfx[r] : pr;
+                    const bool has = ci < n_cand;
+                    const int src = has ? nth_set_bit(pbr, ci - pr) : lane;
+                    int L = -1;
+                    double v = 0.0;
+#pragma unroll
+                    for (int r = 0; r < kPrefetch; ++r) {
+                        const int Lr = __shfl_sync(0xFFFFFFFFu, loc[r], src);
+                        const double vr = __shfl_sync(0xFFFFFFFFu, vv[r], src);
+                        if (r == r_c) {
+                            L = Lr;
+                            v = vr;
+                        }
+                    }
+                    bool emit = false, follower = false;
+                    int phase = 0;
+                    int ow = 0, l = 0, word = 0;
+                    uint32_t term = 0;
+                    if (has) {
+                        ow = L / (kBatch * 1024);
+                        l = L % (kBatch * 1024);
+                        word = l >> 5;
+                        term = chunk_word(it0 + gridDim.x * static_cast<uint32_t>(ow) +
+                                              static_cast<uint32_t>(word >> 5) * geo.n_warps,
+                                          word & 31, geo.nchunks) * 32 +
+                               static_cast<uint32_t>(l & 31);
+                        follower = (s_foll[ow][word] >> (l & 31)) & 1u;
+                        const double av = fabs(v);
+                        uint64_t m[W], p[W];
+                        load_key<W>(st.keys, term, m);
+                        int mpop = 0, ov = 0;
+#pragma unroll
+                        for (int w = 0; w < W; ++w) {
+                            const uint64_t gw = gd.g[w];
+                            p[w] = m[w] ^ gw;
+                            mpop += __popcll(m[w]);
+                            ov += __popcll(m[w] & gw);
+                        }
+                        const int ppop = mpop + gpop - 2 * ov;
+                        bool keep;
+                        if constexpr ((EXT & 2) != 0) keep = keep_partner_mapped<W>(p, tr);
+                        else keep = keep_partner<W>(p, ppop, tr);
+                        if (keep || (tr.has_upper && sinabs * av >= tr.upper)) {
+                            emit = true;
+                            phase = rotation_phase<W, BASIS>(m, p, gd, mpop, ppop);
                         }
                     }
                     const uint32_t eb = __ballot_sync(0xFFFFFFFFu, emit);
@@ -336,7 +388,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                     qb = __shfl_sync(0xFFFFFFFFu, qb, 0);
                     if (emit) {
                         const uint64_t q = qbase + qb + __popc(eb & lt_mask);
-                        sc.q_src[q] = static_cast<uint32_t>(term);
+                        sc.q_src[q] = term;
                         sc.q_flag[q] = static_cast<uint8_t>((follower ? 1 : 0) | (phase_code(phase) << 1));
                         sc.q_val[q] = v;
                         if (!follower) atomicOr(&s_emit[ow][word], 1u << (l & 31));
