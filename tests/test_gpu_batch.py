@@ -70,12 +70,17 @@ def test_batch_gradients_match_single_instance():
 
 def test_autotuner_picks_a_measured_configuration(tmp_path):
     batch = small_batch(16, seed=5)
-    tuner = Autotuner(cache_path=str(tmp_path / "tune.json"), sample=6)
+    tuner = Autotuner(cache_path=str(tmp_path / "tune.json"), sample=6, validate=12)
     best, entry = tuner.tune(batch)
     assert len(entry["table"]) == len(Autotuner.WORKERS) * len(Autotuner.BLOCKS_PER_SM) * len(Autotuner.TABLE_SHIFT)
-    assert min(row["seconds"] for row in entry["table"]) == min(
-        row["seconds"] for row in entry["table"] if row["workers"] == best.workers
-        and row["blocks_per_sm"] == best.blocks_per_sm and row["table_shift"] == best.table_shift)
+    # second stage: the three fastest of the first and the defaults, re-timed on 12 instances
+    keys = ("workers", "blocks_per_sm", "table_shift")
+    val = entry["validation"]
+    assert entry["validation_sample"] == 12 and BatchConfig().as_dict() in [{k: r[k] for k in keys} for r in val]
+    top = sorted(entry["table"], key=lambda row: row["seconds"])[: Autotuner.FINALISTS]
+    assert all({k: r[k] for k in keys} in [{k: v[k] for k in keys} for v in val] for r in top)
+    fastest = min(val, key=lambda row: row["seconds"])
+    assert best == BatchConfig(**{k: fastest[k] for k in keys})
     again, _ = tuner.tune(batch)  # served from the cache
     assert again == best
     r = run_batch(batch, best)
