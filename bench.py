@@ -571,7 +571,8 @@ def batch_bench(args) -> None:
                        "angles": int(sum(wl.n_layers for wl in batch)),
                        "final_terms_max": int(max(int(x) for x in tuned[0].final_terms))},
             "autotuned": {**best.as_dict(), "seconds": t_tuned, "tuning_seconds": tune_s,
-                          "candidates": entry["table"]},
+                          "candidates": entry["table"], "validation": entry.get("validation"),
+                          "validation_sample": entry.get("validation_sample")},
             "default": {**BatchConfig().as_dict(), "seconds": t_default},
             "forward_only": {"value": n / t_fwd, "unit": "expectations/s", "seconds": t_fwd},
             "e2e": {"value": n / t_tuned, "unit": "gradients/s",

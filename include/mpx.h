@@ -173,9 +173,15 @@ MPX_API mpx_status mpx_graph_replay_count(mpx_engine *e, uint64_t *out);
  * the evolved operator. mpx_adjoint_backward replays each segment from its checkpoint and returns
  * grad_angles[l] = d<0|O|0>/d(angle_l) for every circuit layer l, angle_l = theta[map_l] * g_l (host
  * buffer of c's n_layers doubles). Peak extra memory: the checkpoints plus, for the largest segment,
- * 12 bytes per anticommuting term-gate pair and 25 bytes per emitted sine branch. */
+ * 12 bytes per anticommuting term-gate pair and 25 bytes per emitted sine branch. Once an engine has run
+ * one gradient forward pass it knows how many undo records the circuit needs; when they (12 bytes each,
+ * plus 16 bytes per recorded pair) fit in free device memory with room to spare, the next forward pass
+ * logs them all and mpx_adjoint_backward runs the reverse sweep alone, without replaying segments
+ * (mpx_adjoint_logged reports which). The gradient is the same either way. */
 MPX_API mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t segment_gates, double *expectation);
 MPX_API mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *grad_angles);
+/* *out = 1 if the last mpx_adjoint_forward logged everything the reverse sweep needs, else 0. */
+MPX_API mpx_status mpx_adjoint_logged(mpx_engine *e, int32_t *out);
 
 /* Batch of independent problems (observable + circuit + angles each) on one GPU. No reference
  * counterpart: the reference runs one propagator per process (its benches loop over instances). Items

@@ -28,7 +28,7 @@ EXPORTED = ("mpx_create", "mpx_propagate", "mpx_circuit_upload", "mpx_circuit_se
             "mpx_trim_device_memory", "mpx_last_error",
             "mpx_destroy", "mpx_expectation_noalloc", "mpx_batch_run", "mpx_update_initial_operator", "mpx_memory",
             "mpx_graph_info", "mpx_clone", "mpx_current_device", "mpx_graph_pare", "mpx_set_cutoff_type",
-            "mpx_graph_replay_count")
+            "mpx_graph_replay_count", "mpx_adjoint_logged")
 
 
 class MpxError(RuntimeError):
@@ -116,6 +116,7 @@ def load() -> C.CDLL:
             "mpx_graph_pare": (st, [vp, vp, C.c_double]),
             "mpx_set_cutoff_type": (st, [vp, C.c_int32]),
             "mpx_graph_replay_count": (st, [vp, C.POINTER(u64)]),
+            "mpx_adjoint_logged": (st, [vp, C.POINTER(C.c_int32)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -293,6 +294,12 @@ class Engine:
         out = C.c_uint64(0)
         self._check(self.lib.mpx_graph_replay_count(self.h, C.byref(out)))
         return int(out.value)
+
+    def adjoint_logged(self) -> bool:
+        """Whether the last adjoint_forward logged everything the reverse sweep needs (no segment replay)."""
+        out = C.c_int32(0)
+        self._check(self.lib.mpx_adjoint_logged(self.h, C.byref(out)))
+        return bool(out.value)
 
     def adjoint_forward(self, circuit: Circuit, segment_gates: int = 0) -> float:
         """Reset, propagate ``circuit`` saving coefficient checkpoints every ``segment_gates`` gates; <O>."""

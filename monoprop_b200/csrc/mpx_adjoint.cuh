@@ -50,6 +50,18 @@ struct Tape {
     int8_t *r_code;
     uint64_t *r_begin;
     uint64_t r_cap;
+    // forward pass of a gradient that logs everything the reverse sweep needs (no segment replay): both
+    // pre-gate values of every recorded pair, and the undo log (index, pre-gate value of every
+    // anticommuting term, pair members included). Each sweep block reserves its batch's records with one
+    // bump of f_utotal; the next gate's resolve stores where the step's records end (f_ubegin[step + 1]).
+    // Records past f_ucap are counted but not written (the log is then unusable).
+    double *r_vs;
+    double *r_vt;
+    uint32_t *f_uidx;
+    double *f_uval;
+    unsigned long long *f_utotal;
+    uint64_t *f_ubegin;
+    uint64_t f_ucap;
 };
 
 // Per step of a segment: exclusive prefix over the sweep warps' anticommuting counts -> undo offsets

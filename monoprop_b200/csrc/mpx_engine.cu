@@ -67,6 +67,15 @@ struct AdjointState {
     // only_rotate_len_k of the forward pass (0: none) and its outside-set bits over the final store
     uint32_t len_k = 0;
     uint32_t *longb = nullptr;
+    // a forward pass that logged everything the reverse sweep needs (log_ok: nothing overflowed): both
+    // pre-gate values of every recorded pair and the undo log; f_ubegin[st] = first undo record of step st
+    double *r_vs = nullptr, *r_vt = nullptr;
+    uint32_t *f_uidx = nullptr;
+    double *f_uval = nullptr;
+    unsigned long long *f_utotal = nullptr;
+    uint64_t *f_ubegin = nullptr;
+    uint64_t f_ucap = 0;
+    bool log_ok = false;
 };
 
 // A frozen structure (the surrogate "graph" of the reference's variational loop): every gate's rotated
@@ -147,6 +156,7 @@ struct mpx_engine {
     std::vector<GraphEntry> graphs;
     uint64_t store_gen = 0;
     uint64_t rec_hint = 0; // pair records the last recording forward pass needed (sizes the next log)
+    uint64_t undo_hint = 0; // undo records (anticommuting terms over all gates) of the last gradient forward pass
     int64_t pair_log = -1; // mpx_set_pair_log: < 0 automatic, 0 off, > 0 fixed capacity
     uint64_t *d_basis = nullptr; // basis_change rows [2T][W] (tr.basis_rows points here when set)
     // Re-weighted initial operator (mpx_update_initial_operator): store indices and coefficients that
@@ -271,6 +281,27 @@ void release_kept_blocks(int device) {
     }
     if (!out.empty()) cudaStreamSynchronize(nullptr);
     cudaGetLastError();
+}
+
+// Device bytes an allocation of this engine can still get: the device's free memory, the pool's reserved
+// but unused bytes (freed blocks stay reserved: the release threshold is unbounded) and the idle kept
+// blocks of the device (cudaMemGetInfo counts both as used).
+size_t device_available(mpx_engine *e) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    uint64_t reserved = 0, used = 0; // the pool attributes are 64-bit values
+    if (e->pool != nullptr && cudaMemPoolGetAttribute(e->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(e->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+        free_b += static_cast<size_t>(reserved - used);
+    cudaGetLastError();
+    BlockCache &c = block_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    for (const auto &[key, blocks] : c.idle)
+        if (key.first == e->device) free_b += key.second * blocks.size();
+    return free_b;
 }
 
 cudaError_t dev_alloc(mpx_engine *e, void **ptr, size_t bytes) {
@@ -1125,14 +1156,20 @@ void free_adjoint(mpx_engine *e) {
     dev_free(e, e->adj.r_code);
     dev_free(e, e->adj.r_begin);
     dev_free(e, e->adj.longb);
+    for (void *p : {static_cast<void *>(e->adj.r_vs), static_cast<void *>(e->adj.r_vt),
+                    static_cast<void *>(e->adj.f_uidx), static_cast<void *>(e->adj.f_uval),
+                    static_cast<void *>(e->adj.f_utotal), static_cast<void *>(e->adj.f_ubegin)})
+        dev_free(e, p);
     e->adj = AdjointState{};
     e->fwd_tape = Tape{};
 }
 
 // Forward pass for the gradient: resets the store to the initial operator, propagates the circuit
 // segment by segment (segment_gates gates each) and saves the coefficient array at every segment start
-// and at the end.
-mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+// and at the end. With log_all, and when the previous gradient forward pass of this engine says how many
+// undo records the circuit needs and they fit in free device memory, the pass also logs everything the
+// reverse sweep needs (undo log, both values of every pair), so the backward pass replays nothing.
+mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates, bool log_all = false) {
     mpx_engine *e = eng;
     free_adjoint(e);
     mpx_status s = load_initial(e);
@@ -1167,6 +1204,48 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
             cudaGetLastError(); // no room for a log: the backward pass replays with the streaming kernels
         }
     }
+    if (log_all && e->fwd_tape.r_src != nullptr && e->undo_hint > 0) {
+        AdjointState &A = e->adj;
+        const uint64_t u_cap = e->undo_hint + e->undo_hint / 16 + (1ULL << 16);
+        const uint64_t r_cap = e->fwd_tape.r_cap;
+        // large blocks come from power-of-two classes (dev_alloc)
+        const size_t need = next_pow2(u_cap * sizeof(uint32_t)) + next_pow2(u_cap * sizeof(double)) +
+                            2 * next_pow2(r_cap * sizeof(double)) + (L + 2) * sizeof(uint64_t);
+        // headroom for the store's growth and the backward pass's adjoint arrays
+        const size_t reserve = (size_t{4} << 30) + static_cast<size_t>(e->st.cap) * 24;
+        if (need + reserve <= device_available(e)) {
+            cudaError_t ce = dev_alloc(e, reinterpret_cast<void **>(&A.f_uidx), u_cap * sizeof(uint32_t));
+            if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&A.f_uval), u_cap * sizeof(double));
+            if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&A.r_vs), r_cap * sizeof(double));
+            if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&A.r_vt), r_cap * sizeof(double));
+            if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&A.f_utotal), sizeof(unsigned long long));
+            if (ce == cudaSuccess) ce = dev_alloc(e, reinterpret_cast<void **>(&A.f_ubegin), (L + 1) * sizeof(uint64_t));
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(A.f_utotal, 0, sizeof(unsigned long long), e->stream);
+            if (ce == cudaSuccess) ce = cudaMemsetAsync(A.f_ubegin, 0, (L + 1) * sizeof(uint64_t), e->stream);
+            if (ce == cudaSuccess) {
+                A.f_ucap = u_cap;
+                e->fwd_tape.r_vs = A.r_vs;
+                e->fwd_tape.r_vt = A.r_vt;
+                e->fwd_tape.f_uidx = A.f_uidx;
+                e->fwd_tape.f_uval = A.f_uval;
+                e->fwd_tape.f_utotal = A.f_utotal;
+                e->fwd_tape.f_ubegin = A.f_ubegin;
+                e->fwd_tape.f_ucap = u_cap;
+            }
+            else {
+                cudaGetLastError(); // no room after all: the backward pass replays segments
+                for (void *p : {static_cast<void *>(A.r_vs), static_cast<void *>(A.r_vt),
+                                static_cast<void *>(A.f_uidx), static_cast<void *>(A.f_uval),
+                                static_cast<void *>(A.f_utotal), static_cast<void *>(A.f_ubegin)})
+                    dev_free(e, p);
+                A.r_vs = A.r_vt = nullptr;
+                A.f_uidx = nullptr;
+                A.f_uval = nullptr;
+                A.f_utotal = nullptr;
+                A.f_ubegin = nullptr;
+            }
+        }
+    }
     for (uint64_t lo = 0; lo < L; lo += K) {
         double *ck = nullptr;
         MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double)));
@@ -1185,6 +1264,12 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
         e->adj.r_total = e->h_cnt->rec_total;
         e->adj.rec_ok = e->adj.r_total <= e->fwd_tape.r_cap;
         e->rec_hint = std::max(e->rec_hint, e->adj.r_total);
+    }
+    if (e->fwd_tape.f_utotal != nullptr) {
+        unsigned long long u_total = 0;
+        MPX_CUDA(cudaMemcpyAsync(&u_total, e->fwd_tape.f_utotal, sizeof(u_total), cudaMemcpyDeviceToHost, e->stream));
+        MPX_CUDA(cudaStreamSynchronize(e->stream));
+        e->adj.log_ok = e->adj.rec_ok && u_total <= e->adj.f_ucap;
     }
     e->fwd_tape = Tape{};
     if (e->tr.has_len_k) {
@@ -1210,6 +1295,102 @@ mpx_status adjoint_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segme
     MPX_CUDA(cudaStreamSynchronize(e->stream));
     e->last_gates = L;
     e->adj.circuit = &cd;
+    // undo records the circuit needs (every anticommuting term of every gate): sizes the next pass's log
+    uint64_t undo = 0;
+    for (uint64_t st = 0; st < L; ++st) undo += e->adj.stats[4 * st + 1];
+    if (log_all) e->undo_hint = undo;
+    return MPX_OK;
+}
+
+// Reverse sweep over the logs of a forward pass that logged everything (AdjointState::log_ok): no
+// checkpoint, no replay. Pair members keep their undo records (the sweep wrote them before the resolve
+// knew the pairs), so each gate runs the pairs kernel, which marks them done, then the undo kernel.
+mpx_status adjoint_backward_logged(mpx_engine *eng, const CircuitDev &cd, double *grad_angles) {
+    mpx_engine *e = eng;
+    AdjointState &A = e->adj;
+    const uint64_t L = A.L, nf = A.n_final;
+    std::vector<uint64_t> ub(L + 1), rb(L);
+    MPX_CUDA(cudaMemcpyAsync(ub.data(), A.f_ubegin, (L + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaMemcpyAsync(rb.data(), A.r_begin, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
+    std::vector<unsigned long long> cnts(2 * L);
+    for (uint64_t st = 0; st < L; ++st) {
+        cnts[st] = ub[st + 1] - ub[st];
+        cnts[L + st] = (st + 1 < L ? rb[st + 1] : A.r_total) - rb[st];
+    }
+    unsigned long long *d_cnts = nullptr; // u_cnt | p_cnt
+    double *lam = nullptr, *grad = nullptr, *gpart = nullptr;
+    uint32_t *done = nullptr;
+    cudaError_t ce = cudaSuccess;
+    auto A_ = [&](void **ptr, size_t bytes) {
+        if (ce == cudaSuccess) ce = dev_alloc(e, ptr, std::max<size_t>(bytes, 16));
+    };
+    A_(reinterpret_cast<void **>(&d_cnts), 2 * L * sizeof(unsigned long long));
+    A_(reinterpret_cast<void **>(&lam), nf * sizeof(double));
+    A_(reinterpret_cast<void **>(&grad), L * sizeof(double));
+    A_(reinterpret_cast<void **>(&done), ((nf + 31) / 32) * sizeof(uint32_t));
+    A_(reinterpret_cast<void **>(&gpart), (2 * static_cast<size_t>(e->grid) + 1) * sizeof(double));
+    auto release = [&]() {
+        for (void *ptr : {static_cast<void *>(d_cnts), static_cast<void *>(lam), static_cast<void *>(grad),
+                          static_cast<void *>(done), static_cast<void *>(gpart)})
+            dev_free(e, ptr);
+    };
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return fail(eng, MPX_ERR_NOMEM, std::string("gradient allocation failed: ") + cudaGetErrorString(ce));
+    }
+#define MPX_CUDA_REL(call)                                                                                          \
+    do {                                                                                                            \
+        cudaError_t e2_ = (call);                                                                                   \
+        if (e2_ != cudaSuccess) {                                                                                   \
+            release();                                                                                              \
+            return fail(eng, MPX_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e2_));                     \
+        }                                                                                                           \
+    } while (0)
+    MPX_CUDA_REL(cudaMemcpyAsync(d_cnts, cnts.data(), 2 * L * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                 e->stream));
+    MPX_CUDA_REL(cudaMemsetAsync(grad, 0, L * sizeof(double), e->stream));
+    MPX_CUDA_REL(cudaMemsetAsync(done, 0, std::max<uint64_t>((nf + 31) / 32, 1) * sizeof(uint32_t), e->stream));
+    const GradPartials gp{gpart, reinterpret_cast<unsigned int *>(gpart + 2 * static_cast<size_t>(e->grid))};
+    MPX_CUDA_REL(cudaMemsetAsync(gp.arrivals, 0, sizeof(unsigned int), e->stream));
+    if (e->schr) {
+        MPX_CUDA_REL(cudaMemsetAsync(lam, 0, std::max<uint64_t>(nf, 1) * sizeof(double), e->stream));
+        if (e->n_obs > 0 && nf > 0) {
+            pick_lookup(e->W)(e, e->d_obs_keys, e->n_obs, nf, e->d_obs_idx);
+            k_scatter<<<static_cast<unsigned>(std::min<uint64_t>((e->n_obs + 255) / 256, 4096)), 256, 0, e->stream>>>(
+                lam, e->d_obs_idx, e->d_obs_coef, e->n_obs);
+        }
+    }
+    else {
+        pick_adj_init(e->W, e->cfg.basis)(e, lam, 0, nf);
+    }
+    Tape tp{};
+    tp.u_idx = A.f_uidx;
+    tp.u_val = A.f_uval;
+    tp.u_base = A.f_ubegin;
+    tp.u_cnt = d_cnts;
+    tp.p_src = A.r_src;
+    tp.p_tgt = A.r_tgt;
+    tp.p_code = A.r_code;
+    tp.p_vs = A.r_vs;
+    tp.p_vt = A.r_vt;
+    tp.p_base = A.r_begin;
+    tp.p_cnt = d_cnts + L;
+    for (uint64_t st = L; st-- > 0;) {
+        const uint32_t gate = static_cast<uint32_t>(L - 1 - st);
+        launch_dep(e, &k_adj_pairs, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
+                   done, gp);
+        launch_dep(e, &k_adj_undo, tp, static_cast<const GateDesc *>(cd.d_desc), gate, static_cast<uint32_t>(st), lam,
+                   done, gp, grad);
+    }
+    e->launches += 2 * L + 1;
+    MPX_CUDA_REL(cudaGetLastError());
+    MPX_CUDA_REL(cudaMemcpyAsync(grad_angles, grad, L * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    MPX_CUDA_REL(cudaStreamSynchronize(e->stream));
+#undef MPX_CUDA_REL
+    release();
+    MPX_CUDA(cudaStreamSynchronize(e->stream));
     return MPX_OK;
 }
 
@@ -2231,6 +2412,12 @@ mpx_status mpx_launch_count(mpx_engine *e, uint64_t *out) {
     return MPX_OK;
 }
 
+mpx_status mpx_adjoint_logged(mpx_engine *e, int32_t *out) {
+    if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
+    *out = e->adj.log_ok ? 1 : 0;
+    return MPX_OK;
+}
+
 mpx_status mpx_graph_replay_count(mpx_engine *e, uint64_t *out) {
     if (e == nullptr || out == nullptr) return fail(e, MPX_ERR_INVALID, "NULL argument");
     *out = e->graph_replays;
@@ -2250,7 +2437,7 @@ mpx_status mpx_adjoint_forward(mpx_engine *e, const mpx_circuit *c, uint64_t seg
     mpx_engine *eng = e;
     if (c->W != e->W) return fail(eng, MPX_ERR_INVALID, "circuit was uploaded for a different key width");
     MPX_CUDA(cudaSetDevice(e->device));
-    mpx_status s = adjoint_forward(e, *c, segment_gates);
+    mpx_status s = adjoint_forward(e, *c, segment_gates, true);
     if (s != MPX_OK) return s;
     return mpx_expectation(e, expectation);
 }
@@ -2264,6 +2451,12 @@ mpx_status mpx_adjoint_backward(mpx_engine *e, const mpx_circuit *c, double *gra
                                         "with no propagation in between");
     MPX_CUDA(cudaSetDevice(e->device));
     if (c->n == 0) return MPX_OK;
+    if (e->adj.log_ok) {
+        // the forward pass logged everything: the reverse sweep alone
+        const mpx_status s = adjoint_backward_logged(e, *c, grad_angles);
+        if (s == MPX_OK) schr_grad_to_layers(e, grad_angles, c->n);
+        return s;
+    }
     if (!e->adj.rec_ok) {
         // the streaming replay runs with the forward pass's only_rotate_len_k
         const Trunc saved = e->tr;

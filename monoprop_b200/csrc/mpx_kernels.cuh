@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
     __shared__ uint32_t s_wpfx[kWarps + 1]; // their exclusive prefix over the block's warps
     __shared__ uint32_t s_nw[kWarps];       // column words of each warp's current batch
     __shared__ unsigned long long s_ubase[kWarps]; // REPLAY: each warp's undo-log position
+    __shared__ unsigned long long s_fbase;         // logging forward pass: the batch's first undo record
     __shared__ uint32_t s_qn;               // the block's queries so far
     __shared__ uint32_t s_red[kWarps];
     __shared__ uint32_t s_fold[kMaxFoldCols];
@@ -231,6 +232,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                     acc += s_wtot[w];
                 }
                 s_wpfx[kWarps] = acc;
+                if constexpr (!REPLAY) {
+                    if (tp.f_uidx != nullptr)
+                        s_fbase = acc != 0 ? atomicAdd(tp.f_utotal, static_cast<unsigned long long>(acc)) : 0ULL;
+                }
             }
             __syncthreads();
             const int btotal = static_cast<int>(s_wpfx[kWarps]);
@@ -299,6 +304,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                                 tp.u_idx[rr] = kNoStall;
                             }
                         }
+                        else if (!member && tp.f_uidx != nullptr) {
+                            const uint64_t rr = s_fbase + static_cast<uint64_t>(k + kBlock * r + static_cast<int>(threadIdx.x));
+                            if (rr < tp.f_ucap) tp.f_uidx[rr] = kNoStall;
+                        }
                     }
                     if (member) {
                         st.coef[term] = v * cosv;
@@ -309,6 +318,14 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_sweep(Store st, S
                                                                                      static_cast<int>(s_wpfx[ow]));
                             tp.u_idx[rr] = static_cast<uint32_t>(term);
                             tp.u_val[rr] = v;
+                        }
+                        else if (tp.f_uidx != nullptr) {
+                            // logging forward pass: the undo record of this term, in the block's dealing order
+                            const uint64_t rr = s_fbase + static_cast<uint64_t>(k + kBlock * r + static_cast<int>(threadIdx.x));
+                            if (rr < tp.f_ucap) {
+                                tp.f_uidx[rr] = term;
+                                tp.f_uval[rr] = v;
+                            }
                         }
                         if (!(tr.has_lower && sinabs * fabs(v) <= tr.lower)) cand |= 1u << r;
                     }
@@ -628,6 +645,11 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
     }
     const uint32_t stall = cnt->stall;
     const uint64_t n0 = cnt->n0;
+    if constexpr (!REPLAY) {
+        // logging forward pass: this gate's sweep has reserved all its undo records (a stalled step is
+        // re-issued and writes this again)
+        if (tp.f_ubegin != nullptr && blockIdx.x == 0 && threadIdx.x == 0) tp.f_ubegin[step + 1] = *tp.f_utotal;
+    }
     if (stall != kNoStall) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -836,6 +858,7 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                 st.coef[src] = __fma_rn(sinv * -ph, vt0, cs);
                 c_new = (!cos_zero && !LENK) ? __fma_rn(gd.cosv, vt0, (sinv * ph) * v)
                                              : __fma_rn(sinv * ph, v, gd.cosv * vt0);
+                vt = vt0; // the new slot's value before the gate, for a logging forward pass
             }
             st.coef[idx] = c_new;
             const unsigned long long mine = (static_cast<unsigned long long>(tag) << 32) | idx;
@@ -888,6 +911,10 @@ __global__ void __launch_bounds__(kBlock, kSweepBlocksPerSM) k_resolve(Store st,
                         tp.r_src[r] = src;
                         tp.r_tgt[r] = miss ? static_cast<uint32_t>(s_base + off + __popc(ball & lt_mask)) : tgt;
                         tp.r_code[r] = miss ? static_cast<int8_t>(0x10 | (static_cast<int>(ph) & 0xF)) : code;
+                        if (tp.r_vs != nullptr) { // logging forward pass: both values before the gate
+                            tp.r_vs[r] = v;
+                            tp.r_vt[r] = vt;
+                        }
                     }
                 }
             }

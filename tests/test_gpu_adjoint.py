@@ -171,3 +171,44 @@ def test_pair_log_and_replay_agree(make, L):
     assert np.max(np.abs(a[2] - b[2])) <= 1e-10 * max(1.0, np.max(np.abs(b[2])))
     circ.close()
     eng.close()
+
+
+def _logged_case(name):
+    """(workload, layers, only_rotate_len_k) of a logged-backward case."""
+    if name == "ising100_L600":
+        return W.ising100(), 600, None
+    if name == "hubbard6x6_L300":
+        return W.hubbard6x6(), 300, None
+    if name == "hubbard6x6_L300_k4":
+        return W.hubbard6x6(), 300, 4
+    wl = W.line20()  # Schrodinger picture, 200 layers
+    return dataclasses.replace(wl, extra={**wl.extra, "schrodinger_cutoff": 4}), 200, None
+
+
+@pytest.mark.parametrize("name", ["ising100_L600", "hubbard6x6_L300", "hubbard6x6_L300_k4", "line20_L200_s4"])
+def test_logged_backward_equals_replayed_backward(name):
+    """Once an engine knows a circuit's undo-log size, its next gradient forward pass logs everything the
+    reverse sweep needs and the backward pass replays nothing. The gradient is the same as with the segment
+    replay (the logged partner values are the ones the forward pass computed: 1e-12 relative), and <O> too;
+    without a pair log nothing is logged."""
+    wl, L, k = _logged_case(name)
+    eng = _native.engine_for(wl)
+    circ = eng.upload(wl.gen_words()[:L], wl.angles()[:L])
+    eng.set_only_rotate_len_k(k)
+    ev1 = eng.adjoint_forward(circ, 64)
+    assert not eng.adjoint_logged()  # no size known yet: checkpoints and segment replay
+    g1 = eng.adjoint_backward(circ)
+    ev2 = eng.adjoint_forward(circ, 64)
+    assert eng.adjoint_logged()
+    g2 = eng.adjoint_backward(circ)
+    eng.set_pair_log(0)
+    eng.adjoint_forward(circ, 64)
+    assert not eng.adjoint_logged()
+    g3 = eng.adjoint_backward(circ)
+    circ.close()
+    eng.close()
+    assert abs(ev1 - ev2) <= 1e-13 * max(1.0, abs(ev1))
+    scale = max(1.0, float(np.max(np.abs(g1))))
+    assert np.max(np.abs(g2 - g1)) <= 1e-12 * scale
+    assert np.max(np.abs(g3 - g1)) <= 1e-12 * scale
+    assert np.count_nonzero(np.abs(g1) > 1e-9) > 0
