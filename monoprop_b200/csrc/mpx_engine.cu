@@ -1574,8 +1574,9 @@ mpx_status adjoint_backward(mpx_engine *eng, const CircuitDev &cd, double *grad_
         MPX_CUDA_REL(cudaGetLastError());
     }
     e->launches += 1;
-    // the engine keeps the evolved operator of the forward pass
-    if (nf > 0)
+    // the engine keeps the evolved operator of the forward pass (a single segment replayed from the start
+    // has just left it in the store)
+    if (nf > 0 && A.final_coef != nullptr)
         MPX_CUDA_REL(cudaMemcpyAsync(e->st.coef, A.final_coef, nf * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
     MPX_CUDA_REL(cudaMemcpyAsync(e->h_cnt, e->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, e->stream));
     MPX_CUDA_REL(cudaMemcpyAsync(grad_angles, grad, L * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
@@ -1867,11 +1868,11 @@ mpx_status graph_build(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_g
 
 // The frozen structure at the circuit's current angles, from the initial operator; with segment_gates
 // > 0 the coefficient array is saved at segment starts (for the frozen gradient).
-mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+// The values a replay of the frozen structure starts every term of the final store from.
+mpx_status frozen_start(mpx_engine *eng) {
     mpx_engine *e = eng;
     FrozenGraph &g = e->fg;
-    const uint64_t L = g.L, nf = g.n_final;
-    free_adjoint(e);
+    const uint64_t nf = g.n_final;
     if (e->schr) {
         // Schrodinger: the replay starts from the dense reference state, every stored term at its
         // reference-state score, appended terms included (MPOperator.h:169-181)
@@ -1892,6 +1893,45 @@ mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segmen
             MPX_CUDA(cudaMemsetAsync(e->st.coef + e->n_init, 0, (nf - e->n_init) * sizeof(double), e->stream));
     }
     MPX_CUDA(cudaMemsetAsync(g.done, 0, ((nf + 31) / 32) * sizeof(uint32_t), e->stream));
+    return MPX_OK;
+}
+
+// The frozen gradient as one segment whose forward pass is the reverse sweep's own logging replay: only
+// the replay's starting coefficients are saved, and the replay leaves the final state in the store (no
+// separate forward pass).
+mpx_status frozen_single_segment(mpx_engine *eng) {
+    mpx_engine *e = eng;
+    FrozenGraph &g = e->fg;
+    const uint64_t L = g.L, nf = g.n_final;
+    free_adjoint(e);
+    mpx_status s = frozen_start(e);
+    if (s != MPX_OK) return s;
+    const uint64_t n = L > 0 ? g.n0[0] : nf;
+    double *ck = nullptr;
+    MPX_CUDA(dev_alloc(e, reinterpret_cast<void **>(&ck), std::max<uint64_t>(n, 1) * sizeof(double)));
+    e->adj.ck_coef.push_back(ck);
+    if (n > 0) MPX_CUDA(cudaMemcpyAsync(ck, e->st.coef, n * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    e->adj.seg_lo.push_back(0);
+    e->adj.ck_n.push_back(n);
+    e->adj.n_final = nf;
+    e->adj.L = L;
+    e->adj.stats.assign(4 * L, 0);
+    for (uint64_t st = 0; st < L; ++st) {
+        e->adj.stats[4 * st] = g.n0[st];
+        e->adj.stats[4 * st + 1] = g.anti[st];
+        e->adj.stats[4 * st + 2] = g.count[st];
+    }
+    e->adj.w_anti = g.w_anti; // borrowed: released before free_adjoint can see it
+    return MPX_OK;
+}
+
+mpx_status frozen_forward(mpx_engine *eng, const CircuitDev &cd, uint64_t segment_gates) {
+    mpx_engine *e = eng;
+    FrozenGraph &g = e->fg;
+    const uint64_t L = g.L, nf = g.n_final;
+    free_adjoint(e);
+    mpx_status s0 = frozen_start(e);
+    if (s0 != MPX_OK) return s0;
     const Frozen fz = g.view();
     const FrozenFn run = pick_frozen<false>(e->W);
     const uint64_t K = segment_gates == 0 ? std::max<uint64_t>(L, 1) : segment_gates;
@@ -2512,9 +2552,17 @@ mpx_status mpx_graph_gradient(mpx_engine *e, const mpx_circuit *c, uint64_t segm
     mpx_status s = check_graph(e, c);
     if (s != MPX_OK) return s;
     MPX_CUDA(cudaSetDevice(e->device));
-    s = frozen_forward(e, *c, segment_gates == 0 ? std::max<uint64_t>(c->n, 1) : segment_gates);
-    if (s == MPX_OK) s = mpx_expectation(e, expectation);
-    if (s == MPX_OK && c->n > 0) s = adjoint_backward(e, *c, grad_angles, &e->fg);
+    if (segment_gates == 0 && c->n > 0) {
+        // one segment: the reverse sweep's logging replay is the forward pass
+        s = frozen_single_segment(e);
+        if (s == MPX_OK) s = adjoint_backward(e, *c, grad_angles, &e->fg);
+        if (s == MPX_OK) s = mpx_expectation(e, expectation);
+    }
+    else {
+        s = frozen_forward(e, *c, segment_gates == 0 ? std::max<uint64_t>(c->n, 1) : segment_gates);
+        if (s == MPX_OK) s = mpx_expectation(e, expectation);
+        if (s == MPX_OK && c->n > 0) s = adjoint_backward(e, *c, grad_angles, &e->fg);
+    }
     if (s == MPX_OK) schr_grad_to_layers(e, grad_angles, c->n);
     e->adj.w_anti = nullptr; // owned by the graph
     free_adjoint(e);
