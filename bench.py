@@ -21,6 +21,11 @@ sum_g n_g / time.
   index lets the path move fewer bytes than that formula, so ``path_frac`` can exceed 1.
 * ``cpu_baseline``: the unmodified reference engine (compiled from its own sources into
   ``oracle/_ref/libmpref.so``) propagating the same circuit on the host cores.
+* ``gradient``: <O> and the gradient of all 5600 angles per second, two ways: the engine's adjoint of the
+  propagation (``mpx_adjoint_forward`` / ``_backward``) and, under ``graph``, the frozen structure of the
+  reference's variational loop (``mpx_graph_build`` once, then ``mpx_graph_gradient`` per call, what
+  ``_core.expectation_value_and_gradient`` runs); ``cpu_reference`` is the reference's own build_graph +
+  expectation_value_and_gradient on the host cores.
 
 ``--impl reference`` times that reference engine alone on the same workload and prints its own line.
 Multi-GPU (``--gpus N`` under torchrun): N independent replicas of the workload, one per GPU (the
@@ -373,6 +378,32 @@ def main() -> None:
                      "ms_per_eval": g_per, "forward_ms": ms_per_step, "cost_vs_forward": g_per / ms_per_step,
                      "warmup": g_warm, "segment_gates": seg, "n_angles": int(wl.n_layers), "expectation": ev_g,
                      "grad_abs_max": float(np.max(np.abs(grad)))}
+        # The variational loop as the reference runs it (its gradient leg below times the same two calls):
+        # build the frozen structure once, then <O> + gradient of the replayed structure per call (what
+        # _core.expectation_value_and_gradient runs).
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.graph_build(circ)
+        b.record(stream)
+        b.synchronize()
+        build_ms = max_over_ranks(a.elapsed_time(b), dist, dev)
+        gg_ms = []
+        for i in range(g_warm + args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ev_gg, _ = eng.graph_gradient(circ)
+            b.record(stream)
+            b.synchronize()
+            if i >= g_warm:
+                gg_ms.append(a.elapsed_time(b))
+        gg_per = max_over_ranks(sum(gg_ms), dist, dev) / len(gg_ms)
+        grad_line["graph"] = {"value": world * 1e3 / gg_per, "unit": "gradients/s", "ms_per_eval": gg_per,
+                              "build_graph_ms": build_ms, "cost_vs_forward": gg_per / ms_per_step,
+                              "expectation": ev_gg}
 
     # The other two circuits of the task (the 20-qubit line and the 6x6 Hubbard circuit), measured the same
     # way on this GPU (one rank only: no collective takes part).
