@@ -118,6 +118,38 @@ def test_autotuner_sample_is_depth_stratified():
     assert signature(batch).startswith("pauli-W2-c8-support")
 
 
+def test_autotuner_second_stage_overrules_the_small_sample(tmp_path, monkeypatch):
+    """The tuner's choice comes from the second stage: the three fastest configurations of the small sample
+    and the defaults, re-timed on the larger one. Here a fake batch runner makes few workers win on the
+    small sample and lose on the large one (as measured on the 256-instance batched workload), so the
+    defaults must be chosen; the choice is cached."""
+    from monoprop_b200 import batch as B
+
+    calls = []
+
+    class _R:
+        def __init__(self, seconds):
+            self.seconds = seconds
+
+    def fake_run(sample, cfg, gradient=False, segment_gates=0, device=0):
+        calls.append((len(sample), cfg))
+        if len(sample) <= 6:  # small sample: fewer workers look faster
+            return _R(1.0 + 0.1 * cfg.workers + 0.01 * cfg.blocks_per_sm + 0.001 * cfg.table_shift)
+        return _R(10.0 / max(cfg.workers, 1))  # large sample: concurrency pays
+
+    monkeypatch.setattr(B, "run_batch", fake_run)
+    batch = W.batch_ising50(40, seed=4)
+    tuner = B.Autotuner(cache_path=str(tmp_path / "t.json"), sample=6, validate=24)
+    best, entry = tuner.tune(batch)
+    assert len(entry["table"]) == len(B.Autotuner.WORKERS) * len(B.Autotuner.BLOCKS_PER_SM) * len(B.Autotuner.TABLE_SHIFT)
+    finalists = [(r["workers"], r["blocks_per_sm"], r["table_shift"]) for r in entry["validation"]]
+    assert finalists[:3] == [(1, 2, 1), (1, 2, 2), (1, 4, 1)] and (8, 0, 0) in finalists
+    assert entry["validation_sample"] == 24 and best == B.BatchConfig()
+    n_calls = len(calls)
+    again, _ = tuner.tune(batch)  # from the cache: nothing re-timed
+    assert again == best and len(calls) == n_calls
+
+
 def test_basis_rows_encoding():
     """basis_change rows: one row per slot, listed slots set once (indices_to_bitset_checked), zero rows
     above 2 * num_modes, the reference's row-count message."""
